@@ -1,0 +1,107 @@
+/*
+ * mpsw.h — C ABI of the B200 MPAS shallow-water engine (RK4 forward, tangent linear, adjoint).
+ *
+ * The reference exposes its model as the f2py extension module `module_sw_mpas`, object
+ * `mpas_sw_module`: argument-less subroutines acting on module variables that Python reads and
+ * assigns as attributes (src/mpas_sw_module.f90:1-1218, called from src/mpas_sw_driver.py and
+ * demo/run-*.py).  This header is that surface as plain C: one handle holds one module
+ * instance; module variables are read and written by name in the reference's own layout
+ * (Fortran column-major, index arrays 1-based, shapes as var_allocation* gives them); the
+ * subroutines are entry points that run on the current CUDA device.  Handles are not
+ * re-entrant: use one per thread.
+ *
+ * Every function returns 0 on success and a nonzero status otherwise; mpsw_last_error()
+ * describes the failure.  No function aborts the process.
+ */
+#ifndef MPSW_H
+#define MPSW_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mpsw_handle mpsw_handle;
+
+enum {
+  MPSW_OK = 0,
+  MPSW_ERR_ARG = 1,      /* bad argument (unknown name, wrong count, null pointer) */
+  MPSW_ERR_STATE = 2,    /* call out of order (not allocated, mesh not initialised) */
+  MPSW_ERR_MESH = 3,     /* mesh failed validation */
+  MPSW_ERR_CUDA = 4,     /* CUDA runtime error */
+  MPSW_ERR_UNSUPPORTED = 5
+};
+
+/* ---- lifecycle ------------------------------------------------------------------------ */
+/* A new module instance with the reference's default scalars (src/mpas_sw_module.f90:23-55). */
+int mpsw_create(mpsw_handle **out);
+void mpsw_destroy(mpsw_handle *h);
+/* Message of the last failure on this handle (or of mpsw_create when h is NULL). */
+const char *mpsw_last_error(const mpsw_handle *h);
+/* Library version string. */
+const char *mpsw_version(void);
+
+/* ---- module variables (f2py attribute access) ---------------------------------------- */
+/* Scalars: dimensions (nCells, nEdges, ...), config_* switches, logicals as 0/1.  Names are
+ * case-insensitive, as f2py attribute names are.  Constants (a, omega, gravity, pii, ...) are
+ * readable only. */
+int mpsw_set_scalar(mpsw_handle *h, const char *name, double value);
+int mpsw_get_scalar(mpsw_handle *h, const char *name, double *value);
+
+/* Allocatable arrays.  mpsw_var_info reports rank, Fortran dims, element type (0 = double,
+ * 1 = int32) and whether the array is allocated.  mpsw_set_var/mpsw_get_var copy `count`
+ * elements (must equal the allocated size) between a host buffer and the module variable. */
+int mpsw_var_count(void);
+const char *mpsw_var_name(int index);
+int mpsw_var_info(mpsw_handle *h, const char *name, int *rank, long long dims[4], int *is_int,
+                  int *allocated);
+int mpsw_set_var(mpsw_handle *h, const char *name, const void *src, long long count);
+int mpsw_get_var(mpsw_handle *h, const char *name, void *dst, long long count);
+
+/* ---- module subroutines (src/mpas_sw_module.f90) -------------------------------------- */
+int mpsw_var_allocation(mpsw_handle *h);      /* :211-367 */
+int mpsw_var_allocation_tlm(mpsw_handle *h);  /* :369-429 */
+int mpsw_var_allocation_adj(mpsw_handle *h);  /* :431-493 */
+int mpsw_sw_mpas_init_block(mpsw_handle *h);  /* :495-526 */
+int mpsw_sw_rk4(mpsw_handle *h, int nsteps);      /* :528-635, nsteps consecutive calls */
+int mpsw_sw_rk4_tlm(mpsw_handle *h, int nsteps);  /* :637-781 */
+int mpsw_sw_rk4_adj(mpsw_handle *h);              /* :783-1002 */
+
+/* ---- stencil routines on the level-1 state (module diagnostics in and out) ----------- */
+int mpsw_solve_diagnostics(mpsw_handle *h);      /* sw_compute_solve_diagnostics, dyncore.f90:1-361 */
+int mpsw_compute_tend(mpsw_handle *h);           /* sw_compute_tend, dyncore.f90:395-639 */
+int mpsw_reconstruct_2d(mpsw_handle *h);         /* mpas_reconstruct_2d, operators.f90:283-370 */
+int mpsw_solve_diagnostics_tlm(mpsw_handle *h);  /* dyncore_tlm.f90:1-447 */
+int mpsw_compute_tend_tlm(mpsw_handle *h);       /* dyncore_tlm.f90:449-770 */
+int mpsw_reconstruct_2d_tlm(mpsw_handle *h);     /* dyncore_tlm.f90:772-870 */
+/* sw_compute_tend_adj (dyncore_adj.f90:455-738) + mpas_reconstruct_2d_adj (:740-831) +
+ * sw_compute_solve_diagnostics_adj (:1-453) at the level-1 state, as the tail of
+ * link_tlm_adj does them (module.f90:1163-1206): consumes tend_*_ad and the diagnostic /
+ * reconstruction adjoints, accumulates into u_ad(1) and h_ad(1). */
+int mpsw_adjoint_at_state(mpsw_handle *h);
+
+/* ---- device-resident batched path ----------------------------------------------------- */
+/* Member arrays are device buffers laid out [n][B] in the engine's internal (space-filling
+ * curve) order; mpsw_to_internal / mpsw_to_reference convert from/to the reference order.
+ * kind: 0 cells, 1 edges, 2 vertices.  stream: a cudaStream_t (NULL = legacy default). */
+int mpsw_to_internal(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream);
+int mpsw_to_reference(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream);
+
+/* A window of `nsteps` RK4 steps starting from the current level-1 state u(1), h(1) (which is
+ * left unchanged).  The nonlinear trajectory is stored as checkpoints every `ckpt_every`
+ * steps; tangent-linear and adjoint sweeps recompute states and RK stages from them.
+ * precision: 0 = FP64 throughout, 1 = FP32 stencils with FP64 RK accumulation. */
+int mpsw_window_init(mpsw_handle *h, int nsteps, int ckpt_every, void *stream);
+/* Tangent linear over the window, B members in place: du [nEdges][B], dh [nCells][B]. */
+int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh, void *stream);
+/* Adjoint over the window, B members in place: on entry the adjoint of the final state, on
+ * exit the adjoint of the initial state. */
+int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah, void *stream);
+/* Final nonlinear state of the window (device buffers, internal order). */
+int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPSW_H */

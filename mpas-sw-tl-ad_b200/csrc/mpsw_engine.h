@@ -1,0 +1,179 @@
+// Engine behind the C ABI (include/mpsw.h): one module instance, its variables, device mesh,
+// work buffers and the batched tangent-linear / adjoint window.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <initializer_list>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mpsw_internal.h"
+#include "mpsw_setup.h"
+
+namespace mpsw {
+
+struct EngineError : std::runtime_error {
+  int code;
+  EngineError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+std::string lower(const char *s);
+void cuda_check(cudaError_t e, const char *what);
+
+struct Var {
+  std::string name, dims_spec;
+  int group = 0, is_int = 0, ent = 0, mesh = 0, lead = 1;
+  std::vector<long long> dims;
+  long long count = 0;
+  std::vector<double> hr;
+  std::vector<int> hi;
+  double *dev = nullptr;  // [lead][n] internal order (state, diagnostics, tendencies)
+  bool allocated = false, host_valid = true, dev_valid = true;
+  bool nonzero = false;    // may hold nonzero values (adjoint seeds are skipped when false)
+  bool lazy_diag = false;  // device value is produced on demand from the level-1 state
+};
+
+// Storage of the batched tangent-linear / adjoint window (mpsw_window_*).
+struct Window {
+  int nsteps = 0, every = 0, nckpt = 0;
+  std::vector<double *> ck_u, ck_h;    // checkpointed nonlinear states (internal order)
+  double *seg_u = nullptr, *seg_h = nullptr;  // states of one segment, [every][n]
+  double *fin_u = nullptr, *fin_h = nullptr;  // final state
+  // single-trajectory work of the window (FP64)
+  double *x_u = nullptr, *x_h = nullptr;
+  Diag<double> sd[4];
+  double *su[4] = {}, *sh[4] = {};
+  Diag<float> sd32[4];
+  float *su32[4] = {};
+  // member buffers, allocated for the largest B seen
+  int B = 0, prec = -1;
+  std::vector<void *> mem;
+  void *m_diag = nullptr;  // Diag<R> of members (type per prec)
+  void *pu[4] = {}, *ph[4] = {};  // provisional member states / provisional adjoints (R)
+  double *acc_u = nullptr, *acc_h = nullptr;
+  void *adw = nullptr;
+};
+
+struct Engine {
+  std::string err;
+  std::map<std::string, double> scal;
+  std::vector<Var> vars;
+  std::map<std::string, int> index;
+  bool allocated[3] = {false, false, false};
+  int nC = 0, nE = 0, nV = 0, mE = 0, mE2 = 0, vd = 0, nT = 0;
+  cudaStream_t stream = nullptr;
+
+  // device mesh
+  bool mesh_built = false, mesh_dirty = true;
+  BuiltMesh bm;
+  MeshDev<double> m64{};
+  MeshDev<float> m32{};
+  std::vector<void *> mesh_bufs;
+  const int *d_perm[3] = {nullptr, nullptr, nullptr};
+
+  // work
+  std::vector<void *> work;
+  std::vector<double> staging;
+  Diag<double> stage[5]{};
+  Diag<double> tl_diag{};
+  double *sp_u[4] = {}, *sp_h[4] = {}, *tp_u[4] = {}, *tp_h[4] = {};
+  double *acc_u = nullptr, *acc_h = nullptr, *tacc_u = nullptr, *tacc_h = nullptr;
+  AdWork<double> adw{};
+  double *pad_u[2] = {}, *pad_h[2] = {}, *xacc_u = nullptr, *xacc_h = nullptr;
+  int pending_diag = 0;  // 1: diagnostics of the level-1 state owed, 2: and their tangents
+  Window win;
+
+  Engine();
+  ~Engine();
+
+  Var *find(const std::string &lname);
+  Var &var(const char *name);
+  double sc(const char *name) const;
+  long long dim_of(const std::string &sym) const;
+  void need_device();
+  void *dalloc(size_t bytes);
+  void allocate_group(int g);
+  const std::vector<int> &perm_of(int ent) const;
+  void upload(Var &v);
+  void download(Var &v);
+  void set_var(const char *name, const void *src, long long count);
+  void get_var(const char *name, void *dst, long long count);
+  void mark_written(Var &v, bool maybe_nonzero);
+  template <typename T, typename S>
+  const T *up(const std::vector<S> &h, std::vector<void *> &own);
+  template <typename R>
+  void fill_mesh(MeshDev<R> &m);
+  void free_device_mesh();
+  RefMesh ref_mesh();
+  void build_device_mesh();
+  void ensure_mesh();
+  void sync_inputs();
+  void prepare();
+  double *wbuf(size_t n);
+  Diag<double> new_diag(int B);
+  void alloc_work();
+  double *dv(const char *name, int level = 0);
+  Diag<double> module_diag(int g);
+  void mark_diag(int g, bool lazy);
+  void mark_recon(int g);
+  Phys<double> phys() const;
+  void fwd_diag(const double *u, const double *h, const Diag<double> &d, const Phys<double> &ph);
+  void fwd_stage(const double *u, const double *h, const Diag<double> &d, const Phys<double> &ph,
+                 const RK<double, double> &rku, const RK<double, double> &rkh, double *tu, double *th);
+  void tl_diag_run(const Base<double> &bs, const double *ut, const double *ht, const Diag<double> &d,
+                   const Phys<double> &ph);
+  void check_launch(const char *what);
+  void materialize_pending();
+  void finish_levels(std::initializer_list<const char *> names);
+  AdSeeds<double> seeds(bool *any);
+  void zero_ad_seeds();
+  bool recon_seeds_nonzero();
+
+  // module subroutines
+  void init_block();
+  void rk4(int nsteps);
+  void rk4_tlm(int nsteps);
+  void rk4_adj();
+  void solve_diagnostics(int tl);
+  void compute_tend(int tl);
+  void reconstruct(int tl);
+  void adjoint_at_state();
+
+  // batched window (mpsw_window.cu)
+  void window_free();
+  void window_init(int nsteps, int every, cudaStream_t s);
+  void window_tl(int prec, int B, double *du, double *dh, cudaStream_t s);
+  void window_ad(int prec, int B, double *au, double *ah, cudaStream_t s);
+  void window_final(double *u, double *h, cudaStream_t s);
+  void to_internal(int kind, int B, const double *src, double *dst, cudaStream_t s);
+  void to_reference(int kind, int B, const double *src, double *dst, cudaStream_t s);
+};
+
+}  // namespace mpsw
+
+// The opaque handle of the C ABI.
+struct mpsw_handle {
+  mpsw::Engine eng;
+};
+
+namespace mpsw {
+// Runs f on the handle's engine, turning exceptions into status codes (none cross the ABI).
+template <typename F>
+int guarded(mpsw_handle *h, F &&f) {
+  if (!h) return 1;
+  try {
+    f(h->eng);
+    h->eng.err.clear();
+    return 0;
+  } catch (const EngineError &e) {
+    h->eng.err = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    h->eng.err = e.what();
+    return 1;
+  }
+}
+}  // namespace mpsw

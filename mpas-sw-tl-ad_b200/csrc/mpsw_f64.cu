@@ -1,0 +1,27 @@
+// FP64 instantiation of the stencil launchers.  Built with --fmad=false so every multiply and
+// add rounds separately, as in the reference's FP64 Fortran.
+#include "mpsw_launch.cuh"
+
+namespace mpsw {
+
+int grid_for(long long total) {
+  long long g = (total + kThreads - 1) / kThreads;
+  const long long cap = 148LL * 16;  // 16 resident 256-thread blocks on each of the 148 SMs
+  if (g < 1) g = 1;
+  return (int)(g < cap ? g : cap);
+}
+
+void convert_d2f(long long n, const double *src, float *dst, cudaStream_t s) {
+  k_convert<double, float><<<grid_for(n), kThreads, 0, s>>>(n, src, dst);
+}
+void convert_f2d(long long n, const float *src, double *dst, cudaStream_t s) {
+  k_convert<float, double><<<grid_for(n), kThreads, 0, s>>>(n, src, dst);
+}
+
+void convert_list(const ConvList &L, long long max_n, cudaStream_t s) {
+  k_convert_list<<<grid_for(max_n), kThreads, 0, s>>>(L);
+}
+
+template struct Launch<double, double>;
+
+}  // namespace mpsw

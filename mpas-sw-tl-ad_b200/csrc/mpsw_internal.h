@@ -1,0 +1,153 @@
+// Internal data layout of the B200 shallow-water engine.
+//
+// Everything on the device is in *internal order*: cells, edges and vertices are renumbered
+// along a 3-D Hilbert curve of their positions so that neighbour gathers touch nearby
+// addresses; the permutation is applied at the boundary (mpsw_set_var / mpsw_get_var and the
+// to/from-internal kernels), so callers always see the reference's numbering.
+//
+// Connectivity is stored slot-major ([slot][n]) so that, for a fixed slot, consecutive
+// threads read consecutive words.  Gather lists that replace the reference's scatter loops
+// are sorted by the *reference* index of the scattering entity, so each gather performs the
+// same additions in the same order as the reference loop (bit-identical FP64 results).
+//
+// Member arrays (tangent-linear / adjoint batches) are [n][B]: the B members of one cell,
+// edge or vertex are contiguous, so a warp reading one neighbour reads B consecutive values
+// and the connectivity word is a broadcast.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace mpsw {
+
+constexpr int MAXE = 10;   // max edges (and vertices) of a cell
+constexpr int MAXE2 = 20;  // max entries of edgesOnEdge
+constexpr int VDEG = 3;    // vertexDegree (triangular dual mesh)
+
+// Physical constants of the reference (src/mpas_sw_dyncore.f90:414,460).
+constexpr double GRAVITY = 9.80616;
+constexpr double RHO_REF = 1000.0;
+
+template <typename R>
+struct MeshDev {
+  int nC, nE, nV;
+  // cells
+  const int *c_n;              // [N]      nEdgesOnCell
+  const int *c_eoc;            // [MAXE][N] edgesOnCell, reference slot order
+  const int *c_es;             // [MAXE][N] edges of the cell sorted by reference edge index
+  const signed char *c_esg;    // [MAXE][N] +1 if the cell is cellsOnEdge(1) of that edge, else -1
+  const int *c_vs;             // [MAXE][N] vertices of the cell sorted by reference vertex index
+  const R *c_vk;               // [MAXE][N] kiteAreasOnVertex of (that vertex, this cell)
+  const R *c_area;             // [N]
+  const R *c_hs;               // [N]      h_s (bottom topography)
+  const R *c_coef;             // [3][MAXE][N] coeffs_reconstruct
+  const R *c_trig;             // [4][N]   cos(lat), sin(lat), cos(lon), sin(lon)
+  // edges
+  const int *e_c1, *e_c2;      // [E]      cellsOnEdge
+  const int *e_v1, *e_v2;      // [E]      verticesOnEdge
+  const int *e_va, *e_vb;      // [E]      the two vertices listing this edge, reference vertex order
+  const int *e_slot1, *e_slot2;// [E]      slot of this edge in edgesOnCell of cell 1 / cell 2
+  const int *e_n;              // [E]      nEdgesOnEdge
+  const int *e_eoe;            // [MAXE2][E] edgesOnEdge
+  const int *e_rev;            // [MAXE2][E] slot of this edge in the neighbour's edgesOnEdge
+  const R *e_w;                // [MAXE2][E] weightsOnEdge
+  const R *e_dc, *e_dv;        // [E]
+  const R *e_sc2, *e_sc4;      // [E]      meshScalingDel2/Del4
+  const R *e_usrc;             // [E]      u_src
+  // vertices
+  const int *v_es;             // [3][V]   edges of the vertex sorted by reference edge index
+  const signed char *v_esg;    // [3][V]   +1 if the vertex is verticesOnEdge(2) of that edge
+  const int *v_c;              // [3][V]   cellsOnVertex (reference order)
+  const R *v_k;                // [3][V]   kiteAreasOnVertex
+  const int *v_e;              // [3][V]   edgesOnVertex (reference order)
+  const R *v_area, *v_f;       // [V]      areaTriangle, fVertex
+};
+
+// Physics switches and scalars of one configuration (namelist, src/mpas_sw_module.f90:23-42).
+template <typename R>
+struct Phys {
+  R dt, apvm, visc2, visc4;
+  int wind, drag, tc1, sphere;
+};
+
+// Diagnostics of one state (B members, [n][B]); null pointers are not written.
+template <typename R>
+struct Diag {
+  R *circ, *vort, *hv, *pvv;       // vertices
+  R *div, *ke, *pc, *vc;           // cells
+  R *v, *gpt, *pe, *gpn, *he;      // edges
+  R *dsq_u;                        // edges    (del4 only)
+  R *dsq_vort;                     // vertices (del4 only)
+  R *dsq_div;                      // cells    (del4 only)
+};
+
+// Linearisation point of one RK stage (single trajectory, [n]).
+template <typename R>
+struct Base {
+  const R *u, *he, *v, *gpt, *gpn, *pe;  // edges
+  const R *vort, *hv;                    // vertices
+  const R *ke;                           // cells (bottom drag only)
+};
+
+// RK4 bookkeeping of one stage for one prognostic field (src/mpas_sw_module.f90:590-611):
+//   next    = x0 + c * tend   (provisional state of the next stage, omitted at stage 4)
+//   acc_out = acc_in + w * tend
+template <typename R, typename A>
+struct RK {
+  const A *x0;
+  const A *acc_in;
+  A *acc_out;
+  R *next;
+  A c, w;
+  R off;      // next stores x - off (reference-depth offset of the reduced-precision h)
+  int frozen; // test case 1: the wind stays at x0
+};
+
+// Inputs of one adjoint stage: tend_ad = w * x2_ad + c * provis_ad(next stage) + seed.
+template <typename R, typename A>
+struct AdIn {
+  const A *x2u, *x2h;
+  const R *pnu, *pnh;
+  const R *seed_tu, *seed_th;
+  A w, c;
+  int tc1;
+};
+
+// Adjoint seeds of the diagnostics (module *_ad arrays); single member only.
+template <typename R>
+struct AdSeeds {
+  const R *v, *he, *hv, *pe, *pvv, *pc, *circ, *vort, *div, *ke, *vc, *gpn, *gpt;
+};
+
+// Edge/cell/vertex intermediates of one adjoint stage ([n][B]).
+template <typename R>
+struct AdWork {
+  R *pe_ad, *he_ad, *ud, *gpn_ad, *gpt_ad, *v_ad;  // edges
+  R *du_ad;                                       // edges    (del4)
+  R *pc_ad, *ke_ad, *div_ad, *hd;                 // cells
+  R *dd_ad;                                       // cells    (del4)
+  R *hv_ad, *circ_ad;                             // vertices
+  R *dc_ad;                                       // vertices (del4)
+};
+
+// Where the provisional-state adjoint of a stage goes.
+enum AdMode { AD_SET = 0, AD_ADD = 1, AD_FINAL = 2 };
+template <typename R, typename A>
+struct AdOut {
+  R *pad_u, *pad_h;        // provisional adjoint (input of the previous stage), may be null
+  A *acc_u, *acc_h;        // running sum of provisional adjoints
+  const A *x2u, *x2h;      // AD_FINAL: dst = (acc + x2) + pad
+  A *dst_u, *dst_h;
+  int mode;
+};
+
+// Up to kConvMax double arrays rounded to float by one launch (see convert_list).
+constexpr int kConvMax = 10;
+struct ConvList {
+  const double *src[kConvMax];
+  float *dst[kConvMax];
+  long long n[kConvMax];
+  int count;
+};
+
+}  // namespace mpsw

@@ -1,0 +1,55 @@
+// Host-side launchers of the stencil kernels, one instantiation per precision.  The FP64
+// instantiation lives in a translation unit compiled with --fmad=false (bit-identical to the
+// reference arithmetic), the FP32 one in a unit compiled with contraction allowed.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mpsw_internal.h"
+
+namespace mpsw {
+
+int grid_for(long long total);
+
+template <typename R, typename A>
+struct Launch {
+  // forward stage pieces (single trajectory)
+  static void fwd_vertex(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d, cudaStream_t s);
+  static void fwd_cell(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
+                       const RK<R, A> &rk, R *tend_h, cudaStream_t s);
+  static void fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
+                            const Phys<R> &ph, cudaStream_t s);
+  static void del4_vc(const MeshDev<R> &m, int B, const R *dsq_u, R *dsq_vort, R *dsq_div, cudaStream_t s);
+  static void fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
+                            const Phys<R> &ph, const RK<R, A> &rk, R *tend_u, cudaStream_t s);
+  static void tend_h(const MeshDev<R> &m, const R *u, const R *he, R *out, cudaStream_t s);
+  static void recon(const MeshDev<R> &m, int B, int sphere, const R *u, R *X, R *Y, R *Z, R *Zon,
+                    R *Mer, cudaStream_t s);
+  // tangent linear, B members
+  static void tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
+                        const Diag<R> &d, cudaStream_t s);
+  static void tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
+                      const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s);
+  static void tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
+                           const Diag<R> &d, const Phys<R> &ph, cudaStream_t s);
+  static void tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
+                           const Diag<R> &d, const Phys<R> &ph, const RK<R, A> &rk, R *tend_u,
+                           cudaStream_t s);
+  // adjoint of one stage, B members
+  static void ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
+                       const AdIn<R, A> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
+                       const AdOut<R, A> &out, cudaStream_t s);
+  static void recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea, A *u_ad,
+                        cudaStream_t s);
+  // boundary
+  static void to_internal(int n, int B, const int *perm, const double *src, R *dst, cudaStream_t s);
+  static void to_reference(int n, int B, const int *perm, const R *src, double *dst, cudaStream_t s);
+  static void to_internal_acc(int n, int B, const int *perm, const double *src, A *dst, cudaStream_t s);
+  static void to_reference_acc(int n, int B, const int *perm, const A *src, double *dst, cudaStream_t s);
+};
+
+void convert_d2f(long long n, const double *src, float *dst, cudaStream_t s);
+void convert_list(const ConvList &L, long long max_n, cudaStream_t s);
+void convert_f2d(long long n, const float *src, double *dst, cudaStream_t s);
+
+}  // namespace mpsw

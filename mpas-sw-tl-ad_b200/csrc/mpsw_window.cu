@@ -1,0 +1,430 @@
+// Batched tangent-linear / adjoint window of the engine (mpsw_window_* in include/mpsw.h).
+//
+// One nonlinear trajectory (FP64) is shared by B members that ride the trailing dimension of
+// the member arrays.  Per RK stage the trajectory's diagnostics (the linearisation point) are
+// computed once and read by all members; in precision 1 they are rounded to FP32 once per
+// stage and the member stencils run in FP32 while the members' RK4 states and accumulators
+// stay in FP64.
+//
+// Storage of the trajectory: checkpoints every `every` steps; the adjoint sweep replays one
+// segment at a time from its checkpoint (two-level checkpointing: one extra forward pass in
+// total) and recomputes the four RK stages of each step before its adjoint, as
+// src/mpas_sw_module.f90:815-878 does inside sw_rk4_adj.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "mpsw.h"
+#include "mpsw_engine.h"
+#include "mpsw_launch.h"
+
+namespace mpsw {
+
+namespace {
+
+using L64 = Launch<double, double>;
+
+template <typename R>
+struct MemberBufs {
+  Diag<R> d{};
+  R *pu[3] = {}, *ph[3] = {};
+  AdWork<R> w{};
+  R *pad_u[2] = {}, *pad_h[2] = {};
+};
+
+template <typename R>
+R *walloc(Window &W, size_t n, cudaStream_t s) {
+  void *p = nullptr;
+  cuda_check(cudaMalloc(&p, sizeof(R) * (n ? n : 1)), "cudaMalloc window");
+  cuda_check(cudaMemsetAsync(p, 0, sizeof(R) * (n ? n : 1), s), "memset window");
+  W.mem.push_back(p);
+  return (R *)p;
+}
+
+template <typename R>
+MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
+  Window &W = E.win;
+  if (W.m_diag && W.prec == prec && W.B >= B) return (MemberBufs<R> *)W.m_diag;
+  // (re)allocate for this precision and batch
+  for (void *p : W.mem) cudaFree(p);
+  W.mem.clear();
+  delete (MemberBufs<double> *)(W.prec == 0 ? W.m_diag : nullptr);
+  delete (MemberBufs<float> *)(W.prec == 1 ? W.m_diag : nullptr);
+  auto *mb = new MemberBufs<R>();
+  const size_t C = (size_t)E.nC * B, Ed = (size_t)E.nE * B, V = (size_t)E.nV * B;
+  Diag<R> &d = mb->d;
+  d.circ = nullptr;
+  d.vort = walloc<R>(W, V, s); d.hv = nullptr; d.pvv = walloc<R>(W, V, s);
+  d.div = walloc<R>(W, C, s); d.ke = walloc<R>(W, C, s); d.pc = walloc<R>(W, C, s); d.vc = nullptr;
+  d.v = nullptr; d.gpt = nullptr; d.gpn = nullptr;
+  d.pe = walloc<R>(W, Ed, s); d.he = walloc<R>(W, Ed, s);
+  d.dsq_u = walloc<R>(W, Ed, s); d.dsq_vort = walloc<R>(W, V, s); d.dsq_div = walloc<R>(W, C, s);
+  for (int k = 0; k < 3; k++) {
+    mb->pu[k] = walloc<R>(W, Ed, s);
+    mb->ph[k] = walloc<R>(W, C, s);
+  }
+  AdWork<R> &w = mb->w;
+  w.pe_ad = walloc<R>(W, Ed, s); w.he_ad = walloc<R>(W, Ed, s); w.ud = walloc<R>(W, Ed, s);
+  w.gpn_ad = walloc<R>(W, Ed, s); w.gpt_ad = walloc<R>(W, Ed, s); w.v_ad = walloc<R>(W, Ed, s);
+  w.du_ad = walloc<R>(W, Ed, s);
+  w.pc_ad = walloc<R>(W, C, s); w.ke_ad = walloc<R>(W, C, s); w.div_ad = walloc<R>(W, C, s);
+  w.hd = walloc<R>(W, C, s); w.dd_ad = walloc<R>(W, C, s);
+  w.hv_ad = walloc<R>(W, V, s); w.circ_ad = walloc<R>(W, V, s); w.dc_ad = walloc<R>(W, V, s);
+  for (int k = 0; k < 2; k++) {
+    mb->pad_u[k] = walloc<R>(W, Ed, s);
+    mb->pad_h[k] = walloc<R>(W, C, s);
+  }
+  W.acc_u = walloc<double>(W, Ed, s);
+  W.acc_h = walloc<double>(W, C, s);
+  W.m_diag = mb;
+  W.prec = prec;
+  W.B = B;
+  return mb;
+}
+
+Base<double> base64(const Window &W, int k) {
+  const Diag<double> &d = W.sd[k];
+  Base<double> b{};
+  b.u = W.su[k]; b.he = d.he; b.v = d.v; b.gpt = d.gpt; b.gpn = d.gpn; b.pe = d.pe;
+  b.vort = d.vort; b.hv = d.hv; b.ke = d.ke;
+  return b;
+}
+
+Base<float> base32(const Window &W, int k) {
+  const Diag<float> &d = W.sd32[k];
+  Base<float> b{};
+  b.u = W.su32[k]; b.he = d.he; b.v = d.v; b.gpt = d.gpt; b.gpn = d.gpn; b.pe = d.pe;
+  b.vort = d.vort; b.hv = d.hv; b.ke = d.ke;
+  return b;
+}
+
+template <typename R>
+Base<R> base_for(const Window &W, int k);
+template <>
+Base<double> base_for<double>(const Window &W, int k) { return base64(W, k); }
+template <>
+Base<float> base_for<float>(const Window &W, int k) { return base32(W, k); }
+
+template <typename R>
+const MeshDev<R> &mesh_for(const Engine &E);
+template <>
+const MeshDev<double> &mesh_for<double>(const Engine &E) { return E.m64; }
+template <>
+const MeshDev<float> &mesh_for<float>(const Engine &E) { return E.m32; }
+
+template <typename R>
+Phys<R> phys_as(const Phys<double> &p) {
+  Phys<R> q{};
+  q.dt = R(p.dt); q.apvm = R(p.apvm); q.visc2 = R(p.visc2); q.visc4 = R(p.visc4);
+  q.wind = p.wind; q.drag = p.drag; q.tc1 = p.tc1; q.sphere = p.sphere;
+  return q;
+}
+
+void rk_coeffs(double dt, double w[4], double c[4]) {
+  w[0] = dt / 6.; w[1] = dt / 3.; w[2] = dt / 3.; w[3] = dt / 6.;
+  c[0] = dt / 2.; c[1] = dt / 2.; c[2] = dt; c[3] = 0.;
+}
+
+}  // namespace
+
+void Engine::window_free() {
+  Window &W = win;
+  for (void *p : W.mem) cudaFree(p);
+  W.mem.clear();
+  if (W.prec == 0) delete (MemberBufs<double> *)W.m_diag;
+  if (W.prec == 1) delete (MemberBufs<float> *)W.m_diag;
+  W.m_diag = nullptr;
+  W.prec = -1;
+  W.B = 0;
+  for (double *p : W.ck_u) cudaFree(p);
+  for (double *p : W.ck_h) cudaFree(p);
+  W.ck_u.clear();
+  W.ck_h.clear();
+  for (void *p : {(void *)W.seg_u, (void *)W.seg_h, (void *)W.fin_u, (void *)W.fin_h, (void *)W.x_u,
+                  (void *)W.x_h})
+    if (p) cudaFree(p);
+  W.seg_u = W.seg_h = W.fin_u = W.fin_h = W.x_u = W.x_h = nullptr;
+  for (int k = 0; k < 4; k++) {
+    for (double *p : {W.sd[k].circ, W.sd[k].vort, W.sd[k].hv, W.sd[k].pvv, W.sd[k].div, W.sd[k].ke,
+                      W.sd[k].pc, W.sd[k].vc, W.sd[k].v, W.sd[k].gpt, W.sd[k].pe, W.sd[k].gpn,
+                      W.sd[k].he, W.sd[k].dsq_u, W.sd[k].dsq_vort, W.sd[k].dsq_div})
+      if (p) cudaFree(p);
+    for (float *p : {W.sd32[k].vort, W.sd32[k].hv, W.sd32[k].ke, W.sd32[k].v, W.sd32[k].gpt,
+                     W.sd32[k].pe, W.sd32[k].gpn, W.sd32[k].he, W.su32[k]})
+      if (p) cudaFree(p);
+    if (k > 0 && W.su[k]) cudaFree(W.su[k]);
+    if (W.sh[k]) cudaFree(W.sh[k]);
+    W.sd[k] = Diag<double>{};
+    W.sd32[k] = Diag<float>{};
+    W.su[k] = W.sh[k] = nullptr;
+    W.su32[k] = nullptr;
+  }
+  W.nsteps = W.every = W.nckpt = 0;
+}
+
+// One nonlinear FP64 step of the window's trajectory from (x_u, x_h) in place.  With `keep`,
+// the four stages' diagnostics and provisional states are left in sd[k] / su[k] (su[0] is the
+// step's start state) and, in precision 1, rounded to FP32.  tl_hook runs after each stage.
+template <typename Hook>
+static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook) {
+  Window &W = E.win;
+  const Phys<double> ph = E.phys();
+  double w[4], c[4];
+  rk_coeffs(ph.dt, w, c);
+  double *u0 = W.x_u, *h0 = W.x_h;
+  for (int k = 0; k < 4; k++) {
+    W.su[0] = u0;
+    const double *ui = W.su[k];
+    const double *hi = k == 0 ? h0 : W.sh[k];
+    RK<double, double> ru{u0, k == 0 ? u0 : E.acc_u, (k == 3 && in_place) ? u0 : E.acc_u,
+                          k < 3 ? W.su[k + 1] : nullptr, c[k], w[k], 0.0, ph.tc1};
+    RK<double, double> rh{h0, k == 0 ? h0 : E.acc_h, (k == 3 && in_place) ? h0 : E.acc_h,
+                          k < 3 ? W.sh[k + 1] : nullptr, c[k], w[k], 0.0, 0};
+    E.fwd_stage(ui, hi, W.sd[k], ph, ru, rh, nullptr, nullptr);
+    if (prec == 1) {
+      ConvList L{};
+      const Diag<double> &d = W.sd[k];
+      const Diag<float> &f = W.sd32[k];
+      const double *src[] = {ui, d.he, d.v, d.gpt, d.gpn, d.pe, d.vort, d.hv, d.ke};
+      float *dst[] = {W.su32[k], f.he, f.v, f.gpt, f.gpn, f.pe, f.vort, f.hv, f.ke};
+      const long long n[] = {E.nE, E.nE, E.nE, E.nE, E.nE, E.nE, E.nV, E.nV, E.nC};
+      for (int i = 0; i < 9; i++) {
+        L.src[i] = src[i];
+        L.dst[i] = dst[i];
+        L.n[i] = n[i];
+      }
+      L.count = 9;
+      convert_list(L, E.nE, E.stream);
+    }
+    hook(k);
+  }
+}
+
+void Engine::window_init(int nsteps, int every, cudaStream_t s) {
+  if (nsteps < 1 || every < 1) throw EngineError(MPSW_ERR_ARG, "window needs nsteps >= 1 and ckpt_every >= 1");
+  prepare();
+  window_free();
+  Window &W = win;
+  W.nsteps = nsteps;
+  W.every = std::min(every, nsteps);
+  W.nckpt = (nsteps + W.every - 1) / W.every;
+  auto D = [&](size_t n) {
+    void *p = nullptr;
+    cuda_check(cudaMalloc(&p, sizeof(double) * n), "cudaMalloc window");
+    return (double *)p;
+  };
+  auto F = [&](size_t n) {
+    void *p = nullptr;
+    cuda_check(cudaMalloc(&p, sizeof(float) * n), "cudaMalloc window");
+    return (float *)p;
+  };
+  for (int i = 0; i < W.nckpt; i++) {
+    W.ck_u.push_back(D(nE));
+    W.ck_h.push_back(D(nC));
+  }
+  W.seg_u = D((size_t)W.every * nE);
+  W.seg_h = D((size_t)W.every * nC);
+  W.fin_u = D(nE);
+  W.fin_h = D(nC);
+  W.x_u = D(nE);
+  W.x_h = D(nC);
+  for (int k = 0; k < 4; k++) {
+    Diag<double> &d = W.sd[k];
+    d.circ = nullptr; d.vc = nullptr;
+    d.vort = D(nV); d.hv = D(nV); d.pvv = D(nV); d.div = D(nC); d.ke = D(nC); d.pc = D(nC);
+    d.v = D(nE); d.gpt = D(nE); d.pe = D(nE); d.gpn = D(nE); d.he = D(nE);
+    d.dsq_u = D(nE); d.dsq_vort = D(nV); d.dsq_div = D(nC);
+    Diag<float> &f = W.sd32[k];
+    f.vort = F(nV); f.hv = F(nV); f.ke = F(nC); f.v = F(nE); f.gpt = F(nE); f.pe = F(nE);
+    f.gpn = F(nE); f.he = F(nE);
+    W.su32[k] = F(nE);
+    W.su[k] = k == 0 ? nullptr : D(nE);
+    W.sh[k] = k == 0 ? nullptr : D(nC);
+  }
+  // forward over the window from the module's level-1 state, checkpointing
+  cuda_check(cudaStreamSynchronize(s), "window sync");
+  cuda_check(cudaMemcpyAsync(W.x_u, dv("u"), sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "copy");
+  cuda_check(cudaMemcpyAsync(W.x_h, dv("h"), sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "copy");
+  for (int n = 0; n < nsteps; n++) {
+    if (n % W.every == 0) {
+      cuda_check(cudaMemcpyAsync(W.ck_u[n / W.every], W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "ckpt");
+      cuda_check(cudaMemcpyAsync(W.ck_h[n / W.every], W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "ckpt");
+    }
+    traj_step(*this, true, 0, [](int) {});
+  }
+  cuda_check(cudaMemcpyAsync(W.fin_u, W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "final");
+  cuda_check(cudaMemcpyAsync(W.fin_h, W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "final");
+  cuda_check(cudaGetLastError(), "window_init");
+  cuda_check(cudaStreamSynchronize(stream), "window_init");
+}
+
+template <typename R>
+static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
+  Window &W = E.win;
+  MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
+  const MeshDev<R> &m = mesh_for<R>(E);
+  const Phys<double> ph64 = E.phys();
+  const Phys<R> ph = phys_as<R>(ph64);
+  double w[4], c[4];
+  rk_coeffs(ph64.dt, w, c);
+  cuda_check(cudaMemcpyAsync(W.x_u, W.ck_u[0], sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
+  cuda_check(cudaMemcpyAsync(W.x_h, W.ck_h[0], sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
+  for (int n = 0; n < W.nsteps; n++) {
+    traj_step(E, true, prec, [&](int k) {
+      const Base<R> bs = base_for<R>(W, k);
+      const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
+      const R *hti = k == 0 ? nullptr : mb->ph[k - 1];
+      // stage 1 reads the FP64 member state directly when R is double; otherwise round it
+      if (k == 0) {
+        if constexpr (std::is_same<R, double>::value) {
+          uti = du;
+          hti = dh;
+        } else {
+          convert_d2f((long long)E.nE * B, du, mb->pu[2], E.stream);
+          convert_d2f((long long)E.nC * B, dh, mb->ph[2], E.stream);
+          uti = mb->pu[2];
+          hti = mb->ph[2];
+        }
+      }
+      RK<R, double> rut{du, k == 0 ? du : W.acc_u, k == 3 ? du : W.acc_u, k < 3 ? mb->pu[k] : nullptr,
+                        c[k], w[k], R(0), ph.tc1};
+      RK<R, double> rht{dh, k == 0 ? dh : W.acc_h, k == 3 ? dh : W.acc_h, k < 3 ? mb->ph[k] : nullptr,
+                        c[k], w[k], R(0), 0};
+      // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
+      Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, E.stream);
+      Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, E.stream);
+      Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, E.stream);
+      if (ph64.visc4 > 0) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
+      Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, E.stream);
+    });
+  }
+  cuda_check(cudaGetLastError(), "window_tl");
+}
+
+template <typename R>
+static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
+  Window &W = E.win;
+  MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
+  const MeshDev<R> &m = mesh_for<R>(E);
+  const Phys<double> ph64 = E.phys();
+  const Phys<R> ph = phys_as<R>(ph64);
+  double w[4], c[4];
+  rk_coeffs(ph64.dt, w, c);
+  AdSeeds<R> none{};
+  for (int s = W.nckpt - 1; s >= 0; s--) {
+    const int first = s * W.every, len = std::min(W.every, W.nsteps - first);
+    // replay the segment, keeping the start state of every step
+    cuda_check(cudaMemcpyAsync(W.x_u, W.ck_u[s], sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
+    cuda_check(cudaMemcpyAsync(W.x_h, W.ck_h[s], sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
+    for (int j = 0; j < len; j++) {
+      cuda_check(cudaMemcpyAsync(W.seg_u + (size_t)j * E.nE, W.x_u, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "seg");
+      cuda_check(cudaMemcpyAsync(W.seg_h + (size_t)j * E.nC, W.x_h, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "seg");
+      if (j + 1 < len) traj_step(E, true, 0, [](int) {});
+    }
+    for (int j = len - 1; j >= 0; j--) {
+      cuda_check(cudaMemcpyAsync(W.x_u, W.seg_u + (size_t)j * E.nE, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
+      cuda_check(cudaMemcpyAsync(W.x_h, W.seg_h + (size_t)j * E.nC, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
+      // forward sweep of this step, keeping the four stages' linearisation points
+      traj_step(E, false, prec, [](int) {});
+      for (int k = 3; k >= 0; k--) {
+        AdIn<R, double> in{};
+        in.x2u = au; in.x2h = ah; in.w = w[k]; in.c = c[k]; in.tc1 = ph.tc1;
+        in.pnu = k == 3 ? nullptr : mb->pad_u[(k + 1) & 1];
+        in.pnh = k == 3 ? nullptr : mb->pad_h[(k + 1) & 1];
+        AdOut<R, double> out{};
+        out.pad_u = k == 0 ? nullptr : mb->pad_u[k & 1];
+        out.pad_h = k == 0 ? nullptr : mb->pad_h[k & 1];
+        out.acc_u = W.acc_u; out.acc_h = W.acc_h;
+        out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
+        out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
+        Launch<R, double>::ad_stage(m, B, base_for<R>(W, k), ph, in, none, mb->w, out, E.stream);
+      }
+    }
+  }
+  cuda_check(cudaGetLastError(), "window_ad");
+}
+
+static void join(cudaStream_t user, cudaStream_t mine, bool before) {
+  // order the engine stream after (before=true) or before (false) the caller's stream
+  cudaEvent_t ev;
+  cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+  if (before) {
+    cuda_check(cudaEventRecord(ev, user), "event record");
+    cuda_check(cudaStreamWaitEvent(mine, ev, 0), "event wait");
+  } else {
+    cuda_check(cudaEventRecord(ev, mine), "event record");
+    cuda_check(cudaStreamWaitEvent(user, ev, 0), "event wait");
+  }
+  cuda_check(cudaEventDestroy(ev), "event destroy");
+}
+
+void Engine::window_tl(int prec, int B, double *du, double *dh, cudaStream_t s) {
+  if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
+  if (B < 1 || !du || !dh) throw EngineError(MPSW_ERR_ARG, "window_tl needs B >= 1 and member buffers");
+  if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
+  join(s, stream, true);
+  if (prec == 0) window_tl_impl<double>(*this, prec, B, du, dh);
+  else if (prec == 1) window_tl_impl<float>(*this, prec, B, du, dh);
+  else throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+  join(s, stream, false);
+}
+
+void Engine::window_ad(int prec, int B, double *au, double *ah, cudaStream_t s) {
+  if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
+  if (B < 1 || !au || !ah) throw EngineError(MPSW_ERR_ARG, "window_ad needs B >= 1 and member buffers");
+  if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
+  join(s, stream, true);
+  if (prec == 0) window_ad_impl<double>(*this, prec, B, au, ah);
+  else if (prec == 1) window_ad_impl<float>(*this, prec, B, au, ah);
+  else throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+  join(s, stream, false);
+}
+
+void Engine::window_final(double *u, double *h, cudaStream_t s) {
+  if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
+  join(s, stream, true);
+  cuda_check(cudaMemcpyAsync(u, win.fin_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "final u");
+  cuda_check(cudaMemcpyAsync(h, win.fin_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "final h");
+  join(s, stream, false);
+}
+
+void Engine::to_internal(int kind, int B, const double *src, double *dst, cudaStream_t s) {
+  if (!mesh_built) throw EngineError(MPSW_ERR_STATE, "mesh not initialised");
+  if (kind < 0 || kind > 2 || B < 1) throw EngineError(MPSW_ERR_ARG, "bad kind or B");
+  const int n = kind == 0 ? nC : kind == 1 ? nE : nV;
+  L64::to_internal(n, B, d_perm[kind], src, dst, s);
+  cuda_check(cudaGetLastError(), "to_internal");
+}
+
+void Engine::to_reference(int kind, int B, const double *src, double *dst, cudaStream_t s) {
+  if (!mesh_built) throw EngineError(MPSW_ERR_STATE, "mesh not initialised");
+  if (kind < 0 || kind > 2 || B < 1) throw EngineError(MPSW_ERR_ARG, "bad kind or B");
+  const int n = kind == 0 ? nC : kind == 1 ? nE : nV;
+  L64::to_reference(n, B, d_perm[kind], src, dst, s);
+  cuda_check(cudaGetLastError(), "to_reference");
+}
+
+}  // namespace mpsw
+
+// ---- C ABI of the window -----------------------------------------------------------------
+extern "C" {
+int mpsw_to_internal(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.to_internal(kind, B, src, dst, (cudaStream_t)stream); });
+}
+int mpsw_to_reference(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.to_reference(kind, B, src, dst, (cudaStream_t)stream); });
+}
+int mpsw_window_init(mpsw_handle *h, int nsteps, int ckpt_every, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_init(nsteps, ckpt_every, (cudaStream_t)stream); });
+}
+int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_tl(precision, B, du, dh, (cudaStream_t)stream); });
+}
+int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_ad(precision, B, au, ah, (cudaStream_t)stream); });
+}
+int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_final(u, hh, (cudaStream_t)stream); });
+}
+}
