@@ -1,0 +1,410 @@
+"""Benchmark: tangent-linear + adjoint gradients per second of the MPAS shallow-water RK4 model.
+
+Workload (default): level-5 bisected-icosahedron TRiSK mesh (10242 cells, 30720 edges, 20480
+vertices), seeded balanced flow (seed 0), dt = 300 s, a 288-step (24 h) window, trajectory
+checkpointed every 16 steps, perturbations h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s).  One bench step
+is one gradient batch: the nonlinear window with checkpoints, the B-member tangent-linear
+sweep and the B-member adjoint sweep (seeded with the tangent-linear output, i.e. the gradient
+of 1/2 |L dx|^2).  `value` counts gradients of the batched FP32-stencil / FP64-accumulation
+form; the plain FP64 single-member form is timed beside it, with the relative L2 error of the
+batched result against the FP64 window.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--batch B]
+                  [--level L] [--nsteps T]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'mpas-sw-tl-ad_b200'))
+
+METRIC = 'TL+AD gradients/s, batched FP32 vs plain FP64 (rel err<=1e-4)'
+UNIT = 'gradients/s'
+KERNELS = ['tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend', 'ad_edge', 'ad_cell',
+           'ad_vertex', 'ad_final']
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=3)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='mpsw', choices=['mpsw', 'reference'])
+    p.add_argument('--batch', type=int, default=64)
+    p.add_argument('--level', type=int, default=5)
+    p.add_argument('--nsteps', type=int, default=288)
+    p.add_argument('--dt', type=float, default=300.0)
+    p.add_argument('--ckpt', type=int, default=16)
+    p.add_argument('--no-plain', action='store_true', help='skip the plain FP64 arm')
+    return p.parse_args()
+
+
+def workload(level, dt):
+    """Seeded balanced flow (config-0 initial condition) loaded through the module surface."""
+    import numpy as np
+    from mpsw import ic
+    from mpsw.mesh import icosahedral_mesh
+    unit = icosahedral_mesh(level)
+    mesh = ic.scale_mesh(unit)
+    st = ic.balanced_flow(mesh, seed=0)
+    return unit, mesh, st
+
+
+def load_module(mod, unit, mesh, st, dt):
+    import numpy as np
+    mod.nvertlevels = 1
+    mod.ncells, mod.nedges, mod.nvertices = unit['nCells'], unit['nEdges'], unit['nVertices']
+    mod.maxedges, mod.maxedges2, mod.vertexdegree = unit['maxEdges'], unit['maxEdges2'], unit['vertexDegree']
+    mod.r3 = 3
+    mod.ntracers = 1
+    mod.var_allocation()
+    mod.on_a_sphere = True
+    for k in ('latCell', 'lonCell', 'xCell', 'yCell', 'zCell', 'latEdge', 'lonEdge', 'xEdge',
+              'yEdge', 'zEdge', 'latVertex', 'lonVertex', 'xVertex', 'yVertex', 'zVertex',
+              'cellsOnEdge', 'nEdgesOnCell', 'nEdgesOnEdge', 'edgesOnCell', 'edgesOnEdge',
+              'weightsOnEdge', 'dvEdge', 'dcEdge', 'angleEdge', 'areaCell', 'areaTriangle',
+              'cellsOnCell', 'verticesOnCell', 'verticesOnEdge', 'edgesOnVertex', 'cellsOnVertex',
+              'kiteAreasOnVertex', 'meshDensity'):
+        setattr(mod, k.lower(), np.asarray(mesh[k]).T)
+    mod.fvertex = st['fVertex']
+    mod.fedge = st['fEdge']
+    mod.u[0, 0] = st['u']
+    mod.h[0, 0] = st['h']
+    mod.config_dt = dt
+    mod.config_test_case = 7
+    mod.config_apvm_upwinding = 0.5
+
+
+def perturbations(unit, B, seed=1):
+    from mpsw import ic
+    return ic.perturbation(unit, seed, count=B)
+
+
+# ---- reference arm and CPU baseline: the oracle (serial C restatement of the Fortran) -------
+def _oracle_sample(args):
+    """Time `n` forward, tangent-linear and adjoint steps of one member on the host."""
+    level, dt, n, seed = args
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import numpy as np
+    import oracle as O
+    unit, mesh, st = workload(level, dt)
+    m = O.OracleModule()
+    load_module(m, unit, mesh, st, dt)
+    m.var_allocation_tlm()
+    m.var_allocation_adj()
+    m.sw_mpas_init_block()
+    dh, du = perturbations(unit, 1, seed)
+    m.u_tl[0, 0], m.h_tl[0, 0] = du[:, 0], dh[:, 0]
+    u0, h0 = m.u[0, 0].copy(), m.h[0, 0].copy()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        m.sw_rk4()
+    t1 = time.perf_counter()
+    m.u[0, 0], m.h[0, 0] = u0, h0
+    for _ in range(n):
+        m.sw_rk4_tlm()
+    t2 = time.perf_counter()
+    m.u_ad[0, 0], m.h_ad[0, 0] = m.u_tl[0, 0], m.h_tl[0, 0]
+    for _ in range(n):
+        m.u[0, 0], m.h[0, 0] = u0, h0
+        m.sw_rk4_adj()
+    t3 = time.perf_counter()
+    return (t1 - t0) / n, (t2 - t1) / n, (t3 - t2) / n
+
+
+def cpu_gradient_seconds(level, dt, nsteps, sample_steps, workers, pool=None):
+    """Seconds per gradient of the serial reference restatement, from a bounded sample on each
+    of `workers` host processes run concurrently (the slowest process's per-step time,
+    extrapolated linearly to the full window: one forward with trajectory, one TL and one AD
+    sweep)."""
+    t0 = time.perf_counter()
+    if workers == 1 or pool is None:
+        per = [_oracle_sample((level, dt, sample_steps, 1))]
+    else:
+        per = pool.map(_oracle_sample, [(level, dt, sample_steps, 1 + i) for i in range(workers)])
+    wall = time.perf_counter() - t0
+    step_s = max(f + t + a for f, t, a in per)
+    return step_s * nsteps, wall, per
+
+
+def run_reference(a, rank, world):
+    # rank 0 alone times the host baseline; other ranks exit without work
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    workers = os.cpu_count() or 1
+    sample = max(2, min(12, a.nsteps))
+    vals = []
+    with mp.get_context('spawn').Pool(workers) as pool:
+        for i in range(a.warmup + a.steps):
+            sec, wall, per = cpu_gradient_seconds(a.level, a.dt, a.nsteps, 1 if i == 0 else sample,
+                                                  workers, pool)
+            if i >= a.warmup:
+                vals.append(workers / sec)
+    v = statistics.median(vals)
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': a.gpus,
+        'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': 1e3 * workers / v,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh)' % a.level,
+        'config': {'workload': 'TL+AD window, level %d mesh, %d steps of %g s, 1 member per host process' % (a.level, a.nsteps, a.dt)},
+        'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': workers, 'kind': 'port',
+                         'sample': '%d forward + %d TL + %d AD steps per process, extrapolated to %d steps' % (sample, sample, sample, a.nsteps)},
+        'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- clocks -------------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = 'index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap'
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, 'gpurun_out', 'clocks_%d.csv' % os.getpid())
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+# ---- algorithmic bytes of the member kernels ------------------------------------------------------
+def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
+    """Bytes a launch must move if every array element it touches is read or written once.
+    s: bytes of a member / linearisation-point value (8 or 4); accumulators are 8 bytes;
+    connectivity words 4 bytes, mesh metrics s bytes."""
+    a = 8
+    mesh_e = 4 * (nE + sum_eoe) + s * sum_eoe          # nEdgesOnEdge, edgesOnEdge, weights
+    if name == 'tl_edge_tend':
+        mesh = mesh_e + 4 * 4 * nE + 2 * s * nE        # c1,c2,v1,v2; dc,dv
+        base = 3 * s * nE                               # pv_edge, u, h_edge
+        mem = B * (3 * s * nE + 2 * s * nC + 3 * a * nE + s * nE)  # u,pe,he,h,ke; x0,acc r/w; next
+        return mesh + base + mem
+    if name == 'ad_edge':
+        mesh = mesh_e + 4 * sum_eoe + 2 * 4 * nE + s * nE + s * nC   # rev; c1,c2; dv; area
+        base = 6 * s * nE                               # u, h_edge, pv_edge, gradPVn, gradPVt, v
+        mem = B * ((2 * a + s) * nE + (2 * a + s) * nC + 6 * s * nE)  # x2 + next pad (u,h); 6 outputs
+        return mesh + base + mem
+    raise KeyError(name)
+
+
+def run_mpsw(a, rank, world):
+    import numpy as np
+    import torch
+    from module_sw_mpas import MpasSwModule
+    from mpsw import _lib
+    from mpsw.torch_api import FP32, FP64, Engine, Window
+
+    dev = rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    unit, mesh, st = workload(a.level, a.dt)
+    mod = MpasSwModule()
+    load_module(mod, unit, mesh, st, a.dt)
+    mod.var_allocation_tlm()
+    mod.var_allocation_adj()
+    mod.sw_mpas_init_block()
+    eng = Engine(mod)
+    L = _lib.load()
+    B = a.batch
+    nC, nE, nV = unit['nCells'], unit['nEdges'], unit['nVertices']
+    dh_h, du_h = perturbations(unit, B, seed=1 + 1000 * rank)
+    du = torch.tensor(du_h, device='cuda')
+    dh = torch.tensor(dh_h, device='cuda')
+    du_i, dh_i = eng.to_internal(du, 1), eng.to_internal(dh, 0)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+
+    def gradient_batch(prec, Bm, u0, h0):
+        """One bench step on device-resident members: window, TL, AD seeded with the TL output."""
+        w = Window(eng, a.nsteps, a.ckpt)
+        xu, xh = u0.clone(), h0.clone()
+        w.tl_internal(xu, xh, prec)
+        w.ad_internal(xu, xh, prec)
+        return xu, xh
+
+    def timed(fn, n_warm, n_time):
+        for _ in range(n_warm):
+            fn()
+        times = []
+        launches0 = L.mpsw_launch_count()
+        for _ in range(n_time):
+            flush.zero_()  # L2 flush between timed iterations, outside the timed region
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times, (L.mpsw_launch_count() - launches0) / n_time
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+    # batched FP32 stencils / FP64 accumulation: the headline
+    with Clocks(dev) as clk:
+        t32, launches = timed(lambda: gradient_batch(FP32, B, du_i, dh_i), a.warmup, a.steps)
+    clocks = clk.summary()
+    ms = sum(t32) / len(t32)
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], device='cuda', dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * B / (ms / 1e3)
+
+    # accuracy of the batched FP32 form against the FP64 window on the same members
+    ru32, rh32 = gradient_batch(FP32, B, du_i, dh_i)
+    ru64, rh64 = gradient_batch(FP64, B, du_i, dh_i)
+    num = torch.sqrt(((ru32 - ru64) ** 2).sum(0) + ((rh32 - rh64) ** 2).sum(0))
+    den = torch.sqrt((ru64 ** 2).sum(0) + (rh64 ** 2).sum(0))
+    rel_err = float((num / den).max())
+
+    # plain FP64 single-member form (the drop-in numerics, one gradient per sweep)
+    plain = None
+    if not a.no_plain:
+        tp, _ = timed(lambda: gradient_batch(FP64, 1, du_i[:, :1].contiguous(), dh_i[:, :1].contiguous()),
+                      1, max(1, min(a.steps, 2)))
+        plain = 1.0 / (sum(tp) / len(tp) / 1e3)
+
+    # end to end through the public API with host buffers (pinned), copies inside
+    du_host = torch.tensor(du_h).pin_memory()
+    dh_host = torch.tensor(dh_h).pin_memory()
+    out_u = torch.empty_like(du_host).pin_memory()
+    out_h = torch.empty_like(dh_host).pin_memory()
+
+    def e2e_step():
+        w = Window(eng, a.nsteps, a.ckpt)
+        xu = du_host.to('cuda', non_blocking=True)
+        xh = dh_host.to('cuda', non_blocking=True)
+        tu, th = w.tl(xu, xh, FP32)
+        gu, gh = w.ad(tu, th, FP32)
+        out_u.copy_(gu, non_blocking=True)
+        out_h.copy_(gh, non_blocking=True)
+
+    te, _ = timed(e2e_step, 1, a.steps)
+    e2e_val = world * B / (sum(te) / len(te) / 1e3)
+
+    # roofline of the dominant member kernel, timed alone with CUDA events
+    roof = None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json')))
+    except Exception:
+        pass
+    hbm = peaks.get('hbm_gbs')
+    peak_kind = 'measured' if hbm else 'fallback'
+    hbm = hbm or 6650.0
+    gradient_batch(FP32, B, du_i, dh_i)  # leaves the buffers of this configuration in place
+    sum_eoe = int(unit['nEdgesOnEdge'].sum())
+    kt = {}
+    import ctypes
+    for i, name in enumerate(KERNELS):
+        out = ctypes.c_double()
+        eng.h.check(L.mpsw_time_kernel(eng.h.ptr, i, FP32, B, 20, ctypes.byref(out)), 'time_kernel')
+        kt[name] = out.value
+    top = max(('tl_edge_tend', 'ad_edge'), key=lambda k: kt[k])
+    bytes_ = kernel_bytes(top, nC, nE, nV, sum_eoe, B, 4)
+    ach = bytes_ / (kt[top] / 1e3) / 1e9
+    roof = {'bound': 'hbm', 'kernel': top, 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
+            'frac': ach / hbm, 'peak_source': peak_kind, 'traffic': None,
+            'algorithmic_bytes': bytes_, 'ms_per_launch': kt[top],
+            'kernel_ms': kt}
+
+    # host baseline: serial oracle on one core, bounded sample
+    cpu = None
+    if rank == 0:
+        sample = 30
+        sec, wall, per = cpu_gradient_seconds(a.level, a.dt, a.nsteps, sample, 1)
+        cpu = {'value': 1.0 / sec, 'unit': UNIT, 'cores': 1, 'kind': 'port',
+               'sample': '%d forward + %d TL + %d AD steps of one member, extrapolated to %d steps' % (sample, sample, sample, a.nsteps)}
+
+    if rank == 0:
+        wset = (B * (nE + nC) * (8 * 3 + 4 * 12) + 8 * (nE + nC) * 60) / 1e6
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': a.steps,
+            'warmup': a.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32 stencils + f64 accumulation',
+            'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh, seeded perturbations)' % a.level,
+            'config': {'workload': 'TL+AD window: level-%d mesh (%d cells), %d RK4 steps of %g s, %d members, checkpoint every %d' % (a.level, nC, a.nsteps, a.dt, B, a.ckpt),
+                       'members_per_gpu': B, 'parallelism': 'replicas x%d' % world,
+                       'l2': 'flushed (256 MB write) between timed steps; working set ~%.0f MB' % wset},
+            'fp64_plain_gradients_per_s': plain,
+            'batched_vs_plain': (value / world / plain) if plain else None,
+            'rel_err_fp32_vs_fp64': rel_err,
+            'e2e': {'value': e2e_val, 'unit': UNIT, 'h2d_bytes_per_step': int(du_host.numel() * 8 + dh_host.numel() * 8),
+                    'd2h_bytes_per_step': int(out_u.numel() * 8 + out_h.numel() * 8)},
+            'roofline': roof,
+            'cpu_baseline': cpu,
+            'clocks': clocks,
+            'gpu_launches': int(launches),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if a.impl == 'mpsw':
+            torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
+            dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+    if a.impl == 'reference':
+        run_reference(a, rank, world)
+    else:
+        run_mpsw(a, rank, world)
+    if world > 1 and a.impl == 'mpsw':
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -88,6 +88,11 @@ int mpsw_adjoint_at_state(mpsw_handle *h);
 int mpsw_to_internal(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream);
 int mpsw_to_reference(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream);
 
+/* Level-1 prognostic state u(1), h(1) from / to device buffers in the reference order
+ * (nEdges and nCells doubles); the time-2 level and the diagnostics follow as after a step. */
+int mpsw_state_from_device(mpsw_handle *h, const double *u, const double *hh, void *stream);
+int mpsw_state_to_device(mpsw_handle *h, double *u, double *hh, void *stream);
+
 /* A window of `nsteps` RK4 steps starting from the current level-1 state u(1), h(1) (which is
  * left unchanged).  The nonlinear trajectory is stored as checkpoints every `ckpt_every`
  * steps; tangent-linear and adjoint sweeps recompute states and RK stages from them.
@@ -100,6 +105,15 @@ int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh,
 int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah, void *stream);
 /* Final nonlinear state of the window (device buffers, internal order). */
 int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream);
+
+/* ---- measurement ----------------------------------------------------------------------- */
+/* Number of kernels the library has launched in this process (all handles). */
+long long mpsw_launch_count(void);
+/* Average time of `iters` back-to-back launches of one member stencil kernel on the buffers
+ * of the last window sweep (same precision and B): which = 0 tl_vertex, 1 tl_cell,
+ * 2 tl_edge_diag, 3 tl_edge_tend, 4 ad_edge, 5 ad_cell, 6 ad_vertex, 7 ad_final.  Timed with
+ * CUDA events on the engine's stream. */
+int mpsw_time_kernel(mpsw_handle *h, int which, int precision, int B, int iters, double *ms_per_launch);
 
 #ifdef __cplusplus
 }

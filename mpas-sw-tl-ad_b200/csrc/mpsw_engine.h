@@ -48,13 +48,13 @@ struct Window {
   double *su[4] = {}, *sh[4] = {};
   Diag<float> sd32[4];
   float *su32[4] = {};
-  // member buffers, allocated for the largest B seen
-  int B = 0, prec = -1;
-  std::vector<void *> mem;
-  void *m_diag = nullptr;  // Diag<R> of members (type per prec)
-  void *pu[4] = {}, *ph[4] = {};  // provisional member states / provisional adjoints (R)
-  double *acc_u = nullptr, *acc_h = nullptr;
-  void *adw = nullptr;
+  // member buffers per precision (0 FP64, 1 FP32), allocated for the largest B seen
+  struct Members {
+    int B = 0;
+    std::vector<void *> mem;
+    void *bufs = nullptr;  // MemberBufs<R>
+    double *acc_u = nullptr, *acc_h = nullptr;
+  } ms[2];
 };
 
 struct Engine {
@@ -144,10 +144,15 @@ struct Engine {
 
   // batched window (mpsw_window.cu)
   void window_free();
+  void window_free_trajectory();
   void window_init(int nsteps, int every, cudaStream_t s);
+  void window_trajectory(cudaStream_t s);
   void window_tl(int prec, int B, double *du, double *dh, cudaStream_t s);
   void window_ad(int prec, int B, double *au, double *ah, cudaStream_t s);
   void window_final(double *u, double *h, cudaStream_t s);
+  double time_kernel(int which, int prec, int B, int iters);
+  void state_from_device(const double *u, const double *h, cudaStream_t s);
+  void state_to_device(double *u, double *h, cudaStream_t s);
   void to_internal(int kind, int B, const double *src, double *dst, cudaStream_t s);
   void to_reference(int kind, int B, const double *src, double *dst, cudaStream_t s);
 };

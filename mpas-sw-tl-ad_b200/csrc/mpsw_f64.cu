@@ -4,6 +4,8 @@
 
 namespace mpsw {
 
+long long g_launches = 0;
+
 int grid_for(long long total) {
   long long g = (total + kThreads - 1) / kThreads;
   const long long cap = 148LL * 16;  // 16 resident 256-thread blocks on each of the 148 SMs
@@ -12,13 +14,16 @@ int grid_for(long long total) {
 }
 
 void convert_d2f(long long n, const double *src, float *dst, cudaStream_t s) {
+  g_launches++;
   k_convert<double, float><<<grid_for(n), kThreads, 0, s>>>(n, src, dst);
 }
 void convert_f2d(long long n, const float *src, double *dst, cudaStream_t s) {
+  g_launches++;
   k_convert<float, double><<<grid_for(n), kThreads, 0, s>>>(n, src, dst);
 }
 
 void convert_list(const ConvList &L, long long max_n, cudaStream_t s) {
+  g_launches++;
   k_convert_list<<<grid_for(max_n), kThreads, 0, s>>>(L);
 }
 

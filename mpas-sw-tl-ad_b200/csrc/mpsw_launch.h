@@ -10,6 +10,7 @@
 namespace mpsw {
 
 int grid_for(long long total);
+extern long long g_launches;
 
 template <typename R, typename A>
 struct Launch {
@@ -39,6 +40,9 @@ struct Launch {
   static void ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                        const AdIn<R, A> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
                        const AdOut<R, A> &out, cudaStream_t s);
+  // one kernel of ad_stage (0 edge, 1 cell, 2 vertex, 3 final), for timing
+  static void ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
+                      const AdIn<R, A> &in, const AdWork<R> &w, const AdOut<R, A> &out, cudaStream_t s);
   static void recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea, A *u_ad,
                         cudaStream_t s);
   // boundary

@@ -34,52 +34,57 @@ struct MemberBufs {
 };
 
 template <typename R>
-R *walloc(Window &W, size_t n, cudaStream_t s) {
+R *walloc(Window::Members &M, size_t n, cudaStream_t s) {
   void *p = nullptr;
   cuda_check(cudaMalloc(&p, sizeof(R) * (n ? n : 1)), "cudaMalloc window");
   cuda_check(cudaMemsetAsync(p, 0, sizeof(R) * (n ? n : 1), s), "memset window");
-  W.mem.push_back(p);
+  M.mem.push_back(p);
   return (R *)p;
 }
 
 template <typename R>
+void free_members(Window::Members &M) {
+  for (void *p : M.mem) cudaFree(p);
+  M.mem.clear();
+  delete (MemberBufs<R> *)M.bufs;
+  M.bufs = nullptr;
+  M.B = 0;
+  M.acc_u = M.acc_h = nullptr;
+}
+
+template <typename R>
 MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
-  Window &W = E.win;
-  if (W.m_diag && W.prec == prec && W.B >= B) return (MemberBufs<R> *)W.m_diag;
-  // (re)allocate for this precision and batch
-  for (void *p : W.mem) cudaFree(p);
-  W.mem.clear();
-  delete (MemberBufs<double> *)(W.prec == 0 ? W.m_diag : nullptr);
-  delete (MemberBufs<float> *)(W.prec == 1 ? W.m_diag : nullptr);
+  Window::Members &M = E.win.ms[prec];
+  if (M.bufs && M.B >= B) return (MemberBufs<R> *)M.bufs;
+  free_members<R>(M);
   auto *mb = new MemberBufs<R>();
   const size_t C = (size_t)E.nC * B, Ed = (size_t)E.nE * B, V = (size_t)E.nV * B;
   Diag<R> &d = mb->d;
   d.circ = nullptr;
-  d.vort = walloc<R>(W, V, s); d.hv = nullptr; d.pvv = walloc<R>(W, V, s);
-  d.div = walloc<R>(W, C, s); d.ke = walloc<R>(W, C, s); d.pc = walloc<R>(W, C, s); d.vc = nullptr;
+  d.vort = walloc<R>(M, V, s); d.hv = nullptr; d.pvv = walloc<R>(M, V, s);
+  d.div = walloc<R>(M, C, s); d.ke = walloc<R>(M, C, s); d.pc = walloc<R>(M, C, s); d.vc = nullptr;
   d.v = nullptr; d.gpt = nullptr; d.gpn = nullptr;
-  d.pe = walloc<R>(W, Ed, s); d.he = walloc<R>(W, Ed, s);
-  d.dsq_u = walloc<R>(W, Ed, s); d.dsq_vort = walloc<R>(W, V, s); d.dsq_div = walloc<R>(W, C, s);
+  d.pe = walloc<R>(M, Ed, s); d.he = walloc<R>(M, Ed, s);
+  d.dsq_u = walloc<R>(M, Ed, s); d.dsq_vort = walloc<R>(M, V, s); d.dsq_div = walloc<R>(M, C, s);
   for (int k = 0; k < 3; k++) {
-    mb->pu[k] = walloc<R>(W, Ed, s);
-    mb->ph[k] = walloc<R>(W, C, s);
+    mb->pu[k] = walloc<R>(M, Ed, s);
+    mb->ph[k] = walloc<R>(M, C, s);
   }
   AdWork<R> &w = mb->w;
-  w.pe_ad = walloc<R>(W, Ed, s); w.he_ad = walloc<R>(W, Ed, s); w.ud = walloc<R>(W, Ed, s);
-  w.gpn_ad = walloc<R>(W, Ed, s); w.gpt_ad = walloc<R>(W, Ed, s); w.v_ad = walloc<R>(W, Ed, s);
-  w.du_ad = walloc<R>(W, Ed, s);
-  w.pc_ad = walloc<R>(W, C, s); w.ke_ad = walloc<R>(W, C, s); w.div_ad = walloc<R>(W, C, s);
-  w.hd = walloc<R>(W, C, s); w.dd_ad = walloc<R>(W, C, s);
-  w.hv_ad = walloc<R>(W, V, s); w.circ_ad = walloc<R>(W, V, s); w.dc_ad = walloc<R>(W, V, s);
+  w.pe_ad = walloc<R>(M, Ed, s); w.he_ad = walloc<R>(M, Ed, s); w.ud = walloc<R>(M, Ed, s);
+  w.gpn_ad = walloc<R>(M, Ed, s); w.gpt_ad = walloc<R>(M, Ed, s); w.v_ad = walloc<R>(M, Ed, s);
+  w.du_ad = walloc<R>(M, Ed, s);
+  w.pc_ad = walloc<R>(M, C, s); w.ke_ad = walloc<R>(M, C, s); w.div_ad = walloc<R>(M, C, s);
+  w.hd = walloc<R>(M, C, s); w.dd_ad = walloc<R>(M, C, s);
+  w.hv_ad = walloc<R>(M, V, s); w.circ_ad = walloc<R>(M, V, s); w.dc_ad = walloc<R>(M, V, s);
   for (int k = 0; k < 2; k++) {
-    mb->pad_u[k] = walloc<R>(W, Ed, s);
-    mb->pad_h[k] = walloc<R>(W, C, s);
+    mb->pad_u[k] = walloc<R>(M, Ed, s);
+    mb->pad_h[k] = walloc<R>(M, C, s);
   }
-  W.acc_u = walloc<double>(W, Ed, s);
-  W.acc_h = walloc<double>(W, C, s);
-  W.m_diag = mb;
-  W.prec = prec;
-  W.B = B;
+  M.acc_u = walloc<double>(M, Ed, s);
+  M.acc_h = walloc<double>(M, C, s);
+  M.bufs = mb;
+  M.B = B;
   return mb;
 }
 
@@ -130,13 +135,13 @@ void rk_coeffs(double dt, double w[4], double c[4]) {
 
 void Engine::window_free() {
   Window &W = win;
-  for (void *p : W.mem) cudaFree(p);
-  W.mem.clear();
-  if (W.prec == 0) delete (MemberBufs<double> *)W.m_diag;
-  if (W.prec == 1) delete (MemberBufs<float> *)W.m_diag;
-  W.m_diag = nullptr;
-  W.prec = -1;
-  W.B = 0;
+  free_members<double>(W.ms[0]);
+  free_members<float>(W.ms[1]);
+  window_free_trajectory();
+}
+
+void Engine::window_free_trajectory() {
+  Window &W = win;
   for (double *p : W.ck_u) cudaFree(p);
   for (double *p : W.ck_h) cudaFree(p);
   W.ck_u.clear();
@@ -204,11 +209,17 @@ static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook) {
 void Engine::window_init(int nsteps, int every, cudaStream_t s) {
   if (nsteps < 1 || every < 1) throw EngineError(MPSW_ERR_ARG, "window needs nsteps >= 1 and ckpt_every >= 1");
   prepare();
-  window_free();
   Window &W = win;
+  const int ev = std::min(every, nsteps), nck = (nsteps + ev - 1) / ev;
+  if (W.nsteps && W.every == ev && W.nckpt == nck && W.x_u) {
+    W.nsteps = nsteps;  // same storage layout: reuse every buffer
+    window_trajectory(s);
+    return;
+  }
+  window_free_trajectory();
   W.nsteps = nsteps;
-  W.every = std::min(every, nsteps);
-  W.nckpt = (nsteps + W.every - 1) / W.every;
+  W.every = ev;
+  W.nckpt = nck;
   auto D = [&](size_t n) {
     void *p = nullptr;
     cuda_check(cudaMalloc(&p, sizeof(double) * n), "cudaMalloc window");
@@ -242,7 +253,13 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
     W.su[k] = k == 0 ? nullptr : D(nE);
     W.sh[k] = k == 0 ? nullptr : D(nC);
   }
-  // forward over the window from the module's level-1 state, checkpointing
+  window_trajectory(s);
+}
+
+// Forward over the window from the module's level-1 state, checkpointing.
+void Engine::window_trajectory(cudaStream_t s) {
+  Window &W = win;
+  const int nsteps = W.nsteps;
   cuda_check(cudaStreamSynchronize(s), "window sync");
   cuda_check(cudaMemcpyAsync(W.x_u, dv("u"), sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "copy");
   cuda_check(cudaMemcpyAsync(W.x_h, dv("h"), sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "copy");
@@ -287,9 +304,9 @@ static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
           hti = mb->ph[2];
         }
       }
-      RK<R, double> rut{du, k == 0 ? du : W.acc_u, k == 3 ? du : W.acc_u, k < 3 ? mb->pu[k] : nullptr,
+      RK<R, double> rut{du, k == 0 ? du : W.ms[prec].acc_u, k == 3 ? du : W.ms[prec].acc_u, k < 3 ? mb->pu[k] : nullptr,
                         c[k], w[k], R(0), ph.tc1};
-      RK<R, double> rht{dh, k == 0 ? dh : W.acc_h, k == 3 ? dh : W.acc_h, k < 3 ? mb->ph[k] : nullptr,
+      RK<R, double> rht{dh, k == 0 ? dh : W.ms[prec].acc_h, k == 3 ? dh : W.ms[prec].acc_h, k < 3 ? mb->ph[k] : nullptr,
                         c[k], w[k], R(0), 0};
       // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
       Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, E.stream);
@@ -335,7 +352,7 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
         AdOut<R, double> out{};
         out.pad_u = k == 0 ? nullptr : mb->pad_u[k & 1];
         out.pad_h = k == 0 ? nullptr : mb->pad_h[k & 1];
-        out.acc_u = W.acc_u; out.acc_h = W.acc_h;
+        out.acc_u = W.ms[prec].acc_u; out.acc_h = W.ms[prec].acc_h;
         out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
         out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
         Launch<R, double>::ad_stage(m, B, base_for<R>(W, k), ph, in, none, mb->w, out, E.stream);
@@ -405,6 +422,83 @@ void Engine::to_reference(int kind, int B, const double *src, double *dst, cudaS
   cuda_check(cudaGetLastError(), "to_reference");
 }
 
+void Engine::state_from_device(const double *u, const double *h, cudaStream_t s) {
+  prepare();
+  join(s, stream, true);
+  L64::to_internal(nE, 1, d_perm[1], u, dv("u"), stream);
+  L64::to_internal(nC, 1, d_perm[0], h, dv("h"), stream);
+  cuda_check(cudaGetLastError(), "state_from_device");
+  cuda_check(cudaStreamSynchronize(stream), "state_from_device");
+  mark_written(var("u"), true);
+  mark_written(var("h"), true);
+  pending_diag = 1;
+  for (const char *n : {"v", "h_edge", "h_vertex", "pv_edge", "pv_vertex", "pv_cell", "circulation",
+                        "vorticity", "divergence", "ke", "vh", "vorticity_cell", "gradPVn", "gradPVt"}) {
+    mark_written(var(n), true);
+    var(n).lazy_diag = true;
+  }
+}
+
+void Engine::state_to_device(double *u, double *h, cudaStream_t s) {
+  prepare();
+  join(s, stream, true);
+  L64::to_reference(nE, 1, d_perm[1], dv("u"), u, stream);
+  L64::to_reference(nC, 1, d_perm[0], dv("h"), h, stream);
+  cuda_check(cudaGetLastError(), "state_to_device");
+  join(s, stream, false);
+}
+
+template <typename R>
+static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters) {
+  Window &W = E.win;
+  MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
+  const MeshDev<R> &m = mesh_for<R>(E);
+  const Phys<double> ph64 = E.phys();
+  const Phys<R> ph = phys_as<R>(ph64);
+  const Base<R> bs = base_for<R>(W, 1);
+  double w[4], c[4];
+  rk_coeffs(ph64.dt, w, c);
+  RK<R, double> rku{W.ms[prec].acc_u, W.ms[prec].acc_u, W.ms[prec].acc_u, mb->pu[1], c[1], w[1], R(0), 0};
+  RK<R, double> rkh{W.ms[prec].acc_h, W.ms[prec].acc_h, W.ms[prec].acc_h, mb->ph[1], c[1], w[1], R(0), 0};
+  AdIn<R, double> in{};
+  in.x2u = W.ms[prec].acc_u; in.x2h = W.ms[prec].acc_h; in.pnu = mb->pad_u[0]; in.pnh = mb->pad_h[0];
+  in.w = w[1]; in.c = c[1];
+  AdOut<R, double> out{};
+  out.pad_u = mb->pad_u[1]; out.pad_h = mb->pad_h[1];
+  out.acc_u = W.ms[prec].acc_u; out.acc_h = W.ms[prec].acc_h; out.mode = AD_ADD;
+  auto launch = [&]() {
+    using LR = Launch<R, double>;
+    switch (which) {
+      case 0: LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], mb->d, E.stream); break;
+      case 1: LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream); break;
+      case 2: LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream); break;
+      case 3: LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream); break;
+      default: LR::ad_part(which - 4, m, B, bs, ph, in, mb->w, out, E.stream); break;
+    }
+  };
+  launch();  // warm-up
+  cudaEvent_t a, b;
+  cuda_check(cudaEventCreate(&a), "event");
+  cuda_check(cudaEventCreate(&b), "event");
+  cuda_check(cudaEventRecord(a, E.stream), "event");
+  for (int i = 0; i < iters; i++) launch();
+  cuda_check(cudaEventRecord(b, E.stream), "event");
+  cuda_check(cudaEventSynchronize(b), "event");
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, a, b), "event");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cuda_check(cudaGetLastError(), "time_kernel");
+  return (double)ms / iters;
+}
+
+double Engine::time_kernel(int which, int prec, int B, int iters) {
+  if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
+  if (which < 0 || which > 7 || B < 1 || iters < 1) throw EngineError(MPSW_ERR_ARG, "bad kernel timing request");
+  return prec == 1 ? time_kernel_impl<float>(*this, which, prec, B, iters)
+                   : time_kernel_impl<double>(*this, which, prec, B, iters);
+}
+
 }  // namespace mpsw
 
 // ---- C ABI of the window -----------------------------------------------------------------
@@ -423,6 +517,19 @@ int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh,
 }
 int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah, void *stream) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_ad(precision, B, au, ah, (cudaStream_t)stream); });
+}
+int mpsw_state_from_device(mpsw_handle *h, const double *u, const double *hh, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.state_from_device(u, hh, (cudaStream_t)stream); });
+}
+int mpsw_state_to_device(mpsw_handle *h, double *u, double *hh, void *stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.state_to_device(u, hh, (cudaStream_t)stream); });
+}
+long long mpsw_launch_count(void) { return mpsw::g_launches; }
+int mpsw_time_kernel(mpsw_handle *h, int which, int precision, int B, int iters, double *ms_per_launch) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) {
+    if (!ms_per_launch) throw mpsw::EngineError(MPSW_ERR_ARG, "null output");
+    *ms_per_launch = e.time_kernel(which, precision, B, iters);
+  });
 }
 int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_final(u, hh, (cudaStream_t)stream); });

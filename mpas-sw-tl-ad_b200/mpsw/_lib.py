@@ -47,6 +47,10 @@ SIGNATURES = {
     'mpsw_window_tl': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     'mpsw_window_ad': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     'mpsw_window_final_state': (_c_int, [_vp, _vp, _vp, _vp]),
+    'mpsw_state_from_device': (_c_int, [_vp, _vp, _vp, _vp]),
+    'mpsw_state_to_device': (_c_int, [_vp, _vp, _vp, _vp]),
+    'mpsw_launch_count': (_ll, []),
+    'mpsw_time_kernel': (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_c_double)]),
 }
 
 _lib = None

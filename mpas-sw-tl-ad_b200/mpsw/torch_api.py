@@ -1,0 +1,146 @@
+"""PyTorch front end of the engine: device-resident batched windows and the RK4 step as a
+``torch.autograd.Function`` whose backward is the engine's adjoint step.
+
+All tensors are CUDA float64 in the reference numbering: edges ``[nEdges, B]`` for u and
+cells ``[nCells, B]`` for h (members on the trailing dimension).  PyTorch provides device
+memory and the stream; the arithmetic runs in libmpsw.so's kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from ._lib import Handle
+
+FP64, FP32 = 0, 1
+_CELL, _EDGE = 0, 1
+
+
+def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _check_member(t: torch.Tensor, n: int, what: str) -> torch.Tensor:
+    if not (t.is_cuda and t.dtype == torch.float64):
+        raise TypeError(f'{what} must be a CUDA float64 tensor')
+    if t.dim() == 1:
+        t = t.unsqueeze(1)
+    if t.shape[0] != n:
+        raise ValueError(f'{what}: expected {n} rows, got {tuple(t.shape)}')
+    return t.contiguous()
+
+
+class Engine:
+    """Device-side access to one module instance (an ``mpas_sw_module`` after
+    ``sw_mpas_init_block``)."""
+
+    def __init__(self, module):
+        module.sync()
+        self.module = module
+        self.h: Handle = module.handle
+        self.nC = int(module.ncells)
+        self.nE = int(module.nedges)
+
+    # ---- layout -------------------------------------------------------------------------
+    def to_internal(self, x: torch.Tensor, kind: int) -> torch.Tensor:
+        n = self.nE if kind == _EDGE else self.nC
+        x = _check_member(x, n, 'input')
+        out = torch.empty_like(x)
+        self.h.call('mpsw_to_internal', kind, x.shape[1], _ptr(x), _ptr(out), _stream())
+        return out
+
+    def to_reference(self, x: torch.Tensor, kind: int) -> torch.Tensor:
+        n = self.nE if kind == _EDGE else self.nC
+        x = _check_member(x, n, 'input')
+        out = torch.empty_like(x)
+        self.h.call('mpsw_to_reference', kind, x.shape[1], _ptr(x), _ptr(out), _stream())
+        return out
+
+    # ---- state ---------------------------------------------------------------------------
+    def set_state(self, u: torch.Tensor, h: torch.Tensor) -> None:
+        u = _check_member(u, self.nE, 'u')
+        h = _check_member(h, self.nC, 'h')
+        self.h.call('mpsw_state_from_device', _ptr(u), _ptr(h), _stream())
+        self.module.__dict__['_stale'].update({'u', 'h'})
+
+    def get_state(self):
+        u = torch.empty(self.nE, dtype=torch.float64, device='cuda')
+        h = torch.empty(self.nC, dtype=torch.float64, device='cuda')
+        self.h.call('mpsw_state_to_device', _ptr(u), _ptr(h), _stream())
+        return u, h
+
+    # ---- windows -------------------------------------------------------------------------
+    def window(self, nsteps: int, ckpt_every: int = 16) -> 'Window':
+        return Window(self, nsteps, ckpt_every)
+
+
+class Window:
+    """``nsteps`` RK4 steps from the engine's current state, checkpointed every
+    ``ckpt_every`` steps; batched tangent-linear and adjoint sweeps over it."""
+
+    def __init__(self, engine: Engine, nsteps: int, ckpt_every: int = 16):
+        self.e = engine
+        self.nsteps = nsteps
+        engine.h.call('mpsw_window_init', int(nsteps), int(ckpt_every), _stream())
+
+    def final_state(self):
+        u = torch.empty(self.e.nE, 1, dtype=torch.float64, device='cuda')
+        h = torch.empty(self.e.nC, 1, dtype=torch.float64, device='cuda')
+        self.e.h.call('mpsw_window_final_state', _ptr(u), _ptr(h), _stream())
+        return self.e.to_reference(u, _EDGE)[:, 0], self.e.to_reference(h, _CELL)[:, 0]
+
+    def tl_internal(self, du: torch.Tensor, dh: torch.Tensor, precision: int = FP64) -> None:
+        """In place on internal-order members ([nEdges, B], [nCells, B], contiguous)."""
+        B = du.shape[1]
+        self.e.h.call('mpsw_window_tl', int(precision), B, _ptr(du), _ptr(dh), _stream())
+
+    def ad_internal(self, au: torch.Tensor, ah: torch.Tensor, precision: int = FP64) -> None:
+        B = au.shape[1]
+        self.e.h.call('mpsw_window_ad', int(precision), B, _ptr(au), _ptr(ah), _stream())
+
+    def tl(self, du: torch.Tensor, dh: torch.Tensor, precision: int = FP64):
+        """Tangent linear of the window for B members (reference order in and out)."""
+        du_i = self.e.to_internal(du, _EDGE)
+        dh_i = self.e.to_internal(dh, _CELL)
+        self.tl_internal(du_i, dh_i, precision)
+        return self.e.to_reference(du_i, _EDGE), self.e.to_reference(dh_i, _CELL)
+
+    def ad(self, au: torch.Tensor, ah: torch.Tensor, precision: int = FP64):
+        """Adjoint of the window for B members: final-state adjoints in, initial-state out."""
+        au_i = self.e.to_internal(au, _EDGE)
+        ah_i = self.e.to_internal(ah, _CELL)
+        self.ad_internal(au_i, ah_i, precision)
+        return self.e.to_reference(au_i, _EDGE), self.e.to_reference(ah_i, _CELL)
+
+
+class RK4Step(torch.autograd.Function):
+    """One sw_rk4 step (src/mpas_sw_module.f90:528-635) of the state (u, h) as an autograd
+    function; backward runs the engine's adjoint step (:783-1002) linearised at the step's
+    input state.  u, h: CUDA float64 vectors in the reference numbering."""
+
+    @staticmethod
+    def forward(ctx, u, h, engine: Engine):
+        engine.set_state(u, h)
+        w = Window(engine, 1, 1)
+        u1, h1 = w.final_state()
+        ctx.engine = engine
+        ctx.save_for_backward(u, h)
+        return u1, h1
+
+    @staticmethod
+    def backward(ctx, gu, gh):
+        u, h = ctx.saved_tensors
+        e = ctx.engine
+        e.set_state(u, h)
+        w = Window(e, 1, 1)
+        au, ah = w.ad(gu.to(torch.float64).contiguous(), gh.to(torch.float64).contiguous())
+        return au[:, 0], ah[:, 0], None
+
+
+def rk4_step(u, h, engine: Engine):
+    return RK4Step.apply(u, h, engine)

@@ -30,7 +30,29 @@ RECON = ['ureconstructx', 'ureconstructy', 'ureconstructz', 'ureconstructzonal',
 
 
 def pair(level=3, case='tc5', **kw):
-    return setup(O.OracleModule(), level, case, **kw), setup(MpasSwModule(), level, case, **kw)
+    """Oracle and engine module on bit-identical inputs: the oracle builds the case, the
+    engine module receives its arrays through the attribute protocol."""
+    o = setup(O.OracleModule(), level, case, **kw)
+    g = clone(o, MpasSwModule(), **kw)
+    return o, g
+
+
+def clone(o, g, tl=False, ad=False, **cfg):
+    for k in ('ncells', 'nedges', 'nvertices', 'nvertlevels', 'maxedges', 'maxedges2',
+              'vertexdegree', 'r3', 'ntracers', 'config_dt', 'config_test_case',
+              'config_h_mom_eddy_visc2', 'config_h_mom_eddy_visc4', 'config_bottom_drag',
+              'config_wind_stress', 'config_apvm_upwinding', 'on_a_sphere'):
+        setattr(g, k, getattr(o, k))
+    g.var_allocation()
+    if tl:
+        g.var_allocation_tlm()
+    if ad:
+        g.var_allocation_adj()
+    for k, arr in o._arr.items():
+        if g.__dict__['_arr'].get(k) is not None and not k.endswith(('_tl', '_ad')):
+            setattr(g, k, arr)
+    g.sw_mpas_init_block()
+    return g
 
 
 @pytest.mark.parametrize('case', ['tc5', 'seeded', 'tc2', 'tc6'])
