@@ -43,6 +43,8 @@ def parse():
     p.add_argument('--dt', type=float, default=300.0)
     p.add_argument('--ckpt', type=int, default=16)
     p.add_argument('--no-plain', action='store_true', help='skip the plain FP64 arm')
+    p.add_argument('--profile', action='store_true',
+                   help='only the timed batched windows (for profiler launch lists); no JSON line')
     return p.parse_args()
 
 
@@ -285,6 +287,9 @@ def run_mpsw(a, rank, world):
         dist.barrier()
 
     # batched FP32 stencils / FP64 accumulation: the headline
+    if a.profile:
+        timed(lambda: gradient_batch(FP32, B, du_i, dh_i), a.warmup, a.steps)
+        return
     with Clocks(dev) as clk:
         t32, launches = timed(lambda: gradient_batch(FP32, B, du_i, dh_i), a.warmup, a.steps)
     clocks = clk.summary()

@@ -360,6 +360,7 @@ void Engine::fill_mesh(MeshDev<R> &m) {
   m.e_eoe = up<int>(bm.e_eoe, o);
   m.e_rev = up<int>(bm.e_rev, o);
   m.e_w = up<R>(bm.e_w, o);
+  m.e_wrev = up<R>(bm.e_wrev, o);
   m.e_dc = up<R>(bm.e_dc, o);
   m.e_dv = up<R>(bm.e_dv, o);
   m.e_sc2 = up<R>(bm.e_sc2, o);
@@ -426,6 +427,7 @@ void Engine::build_device_mesh() {
   bm = BuiltMesh();
   e = build_mesh(r, g, sfc, &bm);
   if (!e.empty()) throw EngineError(MPSW_ERR_MESH, e);
+  graphs_free();
   free_device_mesh();
   fill_mesh(m64);
   fill_mesh(m32);
@@ -483,7 +485,7 @@ void Engine::alloc_work() {
   adw.gpt_ad = wbuf(nE); adw.v_ad = wbuf(nE); adw.du_ad = wbuf(nE);
   adw.pc_ad = wbuf(nC); adw.ke_ad = wbuf(nC); adw.div_ad = wbuf(nC); adw.hd = wbuf(nC); adw.dd_ad = wbuf(nC);
   adw.hv_ad = wbuf(nV); adw.circ_ad = wbuf(nV); adw.dc_ad = wbuf(nV);
-  for (int k = 0; k < 2; k++) { pad_u[k] = wbuf(nE); pad_h[k] = wbuf(nC); }
+  for (int k = 0; k < 2; k++) { tu_[k] = wbuf(nE); th_[k] = wbuf(nC); }
   xacc_u = wbuf(nE); xacc_h = wbuf(nC);
 }
 
@@ -770,29 +772,33 @@ void Engine::rk4_adj() {  // src/mpas_sw_module.f90:783-1002
   AdSeeds<double> sd = seeds(&any);
   if (any) {
     fwd_diag(u2, h2, stage[0], ph);
-    AdIn<double, double> in{};
-    in.tc1 = 0;
+    cuda_check(cudaMemsetAsync(tu_[0], 0, sizeof(double) * nE, stream), "memset");
+    cuda_check(cudaMemsetAsync(th_[0], 0, sizeof(double) * nC, stream), "memset");
+    AdIn<double> in{tu_[0], th_[0]};
     AdOut<double, double> out{};
     out.acc_u = ua; out.acc_h = ha; out.mode = AD_ADD;
     L64::ad_stage(m64, 1, base_of(stage[0], u2), ph, in, sd, adw, out, stream);
   }
+  // tendency adjoint of stage 4 (:913-914), with any seed left in tend_*_ad
   const double *stu = var("tend_u_ad").nonzero ? dv("tend_u_ad") : nullptr;
   const double *sth = var("tend_h_ad").nonzero ? dv("tend_h_ad") : nullptr;
+  L64::ad_tinit(m64, 1, ua, ha, ph.tc1 ? nullptr : stu, sth, ph.tc1 ? 0.0 : w[3], w[3], tu_[0], th_[0], stream);
   AdSeeds<double> none{};
   for (int k = 3; k >= 0; k--) {  // :912-970
     const double *ui = k == 0 ? u0 : sp_u[k - 1];
-    AdIn<double, double> in{};
-    in.x2u = ua; in.x2h = ha; in.w = w[k]; in.c = c[k]; in.tc1 = ph.tc1;
-    in.pnu = k == 3 ? nullptr : pad_u[(k + 1) & 1];
-    in.pnh = k == 3 ? nullptr : pad_h[(k + 1) & 1];
-    in.seed_tu = k == 3 ? stu : nullptr;
-    in.seed_th = k == 3 ? sth : nullptr;
+    AdIn<double> in{tu_[(3 - k) & 1], th_[(3 - k) & 1]};
     AdOut<double, double> out{};
-    out.pad_u = k == 0 ? nullptr : pad_u[k & 1];
-    out.pad_h = k == 0 ? nullptr : pad_h[k & 1];
     out.acc_u = xacc_u; out.acc_h = xacc_h;
-    out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
     out.x2u = ua; out.x2h = ha; out.dst_u = ua; out.dst_h = ha;
+    out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
+    if (k > 0) {
+      out.tu_next = tu_[(4 - k) & 1];
+      out.th_next = th_[(4 - k) & 1];
+      out.wu = ph.tc1 ? 0.0 : w[k - 1];
+      out.cu = ph.tc1 ? 0.0 : c[k - 1];
+      out.wh = w[k - 1];
+      out.ch = c[k - 1];
+    }
     L64::ad_stage(m64, 1, base_of(stage[k + 1], ui), ph, in, none, adw, out, stream);
   }
   cuda_check(cudaMemsetAsync(dv("u_ad", 1), 0, sizeof(double) * nE, stream), "memset");
@@ -867,10 +873,10 @@ void Engine::adjoint_at_state() {  // src/mpas_sw_module.f90:1163-1206
                    dv("uReconstructZonal_ad"), dv("uReconstructMeridional_ad"), ua, stream);
   bool any = false;
   AdSeeds<double> sd = seeds(&any);
-  AdIn<double, double> in{};
-  in.tc1 = ph.tc1;
-  in.seed_tu = var("tend_u_ad").nonzero ? dv("tend_u_ad") : nullptr;
-  in.seed_th = var("tend_h_ad").nonzero ? dv("tend_h_ad") : nullptr;
+  const double *stu = var("tend_u_ad").nonzero && !ph.tc1 ? dv("tend_u_ad") : nullptr;
+  const double *sth = var("tend_h_ad").nonzero ? dv("tend_h_ad") : nullptr;
+  L64::ad_tinit(m64, 1, nullptr, nullptr, stu, sth, 0.0, 0.0, tu_[0], th_[0], stream);
+  AdIn<double> in{tu_[0], th_[0]};
   AdOut<double, double> out{};
   out.acc_u = ua; out.acc_h = ha; out.mode = AD_ADD;
   L64::ad_stage(m64, 1, base_of(stage[0], u0), ph, in, sd, adw, out, stream);

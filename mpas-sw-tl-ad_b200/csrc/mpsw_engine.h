@@ -57,8 +57,25 @@ struct Window {
   } ms[2];
 };
 
+// A captured CUDA graph of one window step, keyed by what its kernels bake in.
+struct GraphKey {
+  int kind = 0, prec = 0, B = 0;
+  const void *p1 = nullptr, *p2 = nullptr;
+  double dt = 0, apvm = 0, visc2 = 0, visc4 = 0;
+  int flags = 0;
+  bool operator==(const GraphKey &o) const {
+    return kind == o.kind && prec == o.prec && B == o.B && p1 == o.p1 && p2 == o.p2 && dt == o.dt &&
+           apvm == o.apvm && visc2 == o.visc2 && visc4 == o.visc4 && flags == o.flags;
+  }
+};
+struct GraphEntry {
+  GraphKey key;
+  cudaGraphExec_t exec = nullptr;
+};
+
 struct Engine {
   std::string err;
+  std::vector<GraphEntry> graphs;
   std::map<std::string, double> scal;
   std::vector<Var> vars;
   std::map<std::string, int> index;
@@ -82,7 +99,7 @@ struct Engine {
   double *sp_u[4] = {}, *sp_h[4] = {}, *tp_u[4] = {}, *tp_h[4] = {};
   double *acc_u = nullptr, *acc_h = nullptr, *tacc_u = nullptr, *tacc_h = nullptr;
   AdWork<double> adw{};
-  double *pad_u[2] = {}, *pad_h[2] = {}, *xacc_u = nullptr, *xacc_h = nullptr;
+  double *tu_[2] = {}, *th_[2] = {}, *xacc_u = nullptr, *xacc_h = nullptr;
   int pending_diag = 0;  // 1: diagnostics of the level-1 state owed, 2: and their tangents
   Window win;
 
@@ -143,6 +160,10 @@ struct Engine {
   void adjoint_at_state();
 
   // batched window (mpsw_window.cu)
+  void graphs_free();
+  GraphKey graph_key(int kind, int prec, int B, const void *p1, const void *p2) const;
+  template <typename F>
+  void run_graph(const GraphKey &k, F &&body);
   void window_free();
   void window_free_trajectory();
   void window_init(int nsteps, int every, cudaStream_t s);

@@ -51,6 +51,7 @@ struct MeshDev {
   const int *e_eoe;            // [MAXE2][E] edgesOnEdge
   const int *e_rev;            // [MAXE2][E] slot of this edge in the neighbour's edgesOnEdge
   const R *e_w;                // [MAXE2][E] weightsOnEdge
+  const R *e_wrev;             // [MAXE2][E] weight of this edge in the neighbour's list (transpose)
   const R *e_dc, *e_dv;        // [E]
   const R *e_sc2, *e_sc4;      // [E]      meshScalingDel2/Del4
   const R *e_usrc;             // [E]      u_src
@@ -103,14 +104,12 @@ struct RK {
   int frozen; // test case 1: the wind stays at x0
 };
 
-// Inputs of one adjoint stage: tend_ad = w * x2_ad + c * provis_ad(next stage) + seed.
-template <typename R, typename A>
+// Input of one adjoint stage: its tendency adjoint, tu (edges) and th / areaCell (cells), as
+// formed by the previous adjoint stage (or k_ad_tinit) from src/mpas_sw_module.f90:912-942:
+// tend_ad = w * x2_ad + c * provis_ad(next stage) [+ seed].
+template <typename R>
 struct AdIn {
-  const A *x2u, *x2h;
-  const R *pnu, *pnh;
-  const R *seed_tu, *seed_th;
-  A w, c;
-  int tc1;
+  const R *tu, *th;
 };
 
 // Adjoint seeds of the diagnostics (module *_ad arrays); single member only.
@@ -130,15 +129,21 @@ struct AdWork {
   R *dc_ad;                                       // vertices (del4)
 };
 
-// Where the provisional-state adjoint of a stage goes.
+// Where the provisional-state adjoint `pad` of a stage goes.
+//   AD_SET:   acc = pad              AD_ADD: acc = acc + pad
+//   AD_FINAL: dst = (acc + x2) + pad (the step's input adjoint; dst may alias x2)
+// and the tendency adjoint of the stage before it:
+//   tu_next = wu * x2 + cu * pad     (AD_FINAL: wu * dst, the first stage of the next step)
+//   th_next = (wh * x2 + ch * pad) / areaCell
 enum AdMode { AD_SET = 0, AD_ADD = 1, AD_FINAL = 2 };
 template <typename R, typename A>
 struct AdOut {
-  R *pad_u, *pad_h;        // provisional adjoint (input of the previous stage), may be null
-  A *acc_u, *acc_h;        // running sum of provisional adjoints
-  const A *x2u, *x2h;      // AD_FINAL: dst = (acc + x2) + pad
+  A *acc_u, *acc_h;
+  const A *x2u, *x2h;
   A *dst_u, *dst_h;
   int mode;
+  R *tu_next, *th_next;
+  A wu, cu, wh, ch;
 };
 
 // Up to kConvMax double arrays rounded to float by one launch (see convert_list).

@@ -436,46 +436,49 @@ __global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restr
 // as gathers.  tend_ad is formed on the fly from the step-output adjoint and the next
 // stage's provisional adjoint (src/mpas_sw_module.f90:912-942).
 // ----------------------------------------------------------------------------------------
+// Tendency adjoint of the last stage of a step (src/mpas_sw_module.f90:912-914 at rk=4):
+// tu = wu * x2u + seed_tu, th = (wh * x2h + seed_th) / areaCell.  One grid covers E*B edge
+// threads then N*B cell threads.
 template <typename R, typename A>
-__device__ __forceinline__ R ad_tu(const AdIn<R, A> &in, int B, int e, int b) {
-  if (in.tc1) return R(0);
-  A t = A(0);
-  if (in.x2u) t = in.w * in.x2u[(size_t)e * B + b];
-  if (in.pnu) t = t + in.c * A(in.pnu[(size_t)e * B + b]);
-  R r = R(t);
-  if (in.seed_tu) r = r + in.seed_tu[e];
-  return r;
-}
-template <typename R, typename A>
-__device__ __forceinline__ R ad_th(const AdIn<R, A> &in, int B, int c, int b) {
-  A t = A(0);
-  if (in.x2h) t = in.w * in.x2h[(size_t)c * B + b];
-  if (in.pnh) t = t + in.c * A(in.pnh[(size_t)c * B + b]);
-  R r = R(t);
-  if (in.seed_th) r = r + in.seed_th[c];
-  return r;
+__global__ void k_ad_tinit(MeshDev<R> m, int B, const A *x2u, const A *x2h, const R *seed_tu,
+                           const R *seed_th, A wu, A wh, R *tu, R *th) {
+  const int nE = m.nE;
+  const long long te = (long long)nE * B;
+  MPSW_GRID_LOOP(t, te + (long long)m.nC * B) {
+    if (t < te) {
+      const int e = (int)(t / B);
+      A x = x2u ? wu * x2u[t] : A(0);
+      if (seed_tu) x = x + A(seed_tu[e]);
+      tu[t] = R(x);
+    } else {
+      const long long t2 = t - te;
+      const int c = (int)(t2 / B);
+      A x = x2h ? wh * x2h[t2] : A(0);
+      if (seed_th) x = x + A(seed_th[c]);
+      th[t2] = R(x / A(ld(m.c_area, c)));
+    }
+  }
 }
 
 // Edge stage: workpv/q adjoint (:689-718) as a gather over the transposed edgesOnEdge,
 // thickness-flux adjoint (:720-736), drag (:549-565), wind (:567-572), then the APVM adjoints
 // of the diagnostics (:193-200, :235-242).
 template <typename R, typename A>
-__global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A> in, AdSeeds<R> sd,
+__global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                           AdWork<R> w) {
   const int nE = m.nE;
   MPSW_GRID_LOOP(t, (long long)nE * B) {
     const int e = (int)(t / B), b = (int)(t - (long long)e * B);
     const int n = ld(m.e_n, e);
-    const R Te = ad_tu(in, B, e, b);
+    const R Te = in.tu[(size_t)e * B + b];
     const R ue = ld(bs.u, e), hee = ld(bs.he, e), pee = ld(bs.pe, e);
     R pe_ad = R(0), he_ad = R(0), ud = R(0);
     for (int j = 0; j < n; j++) {
       const int nb = ld(m.e_eoe, (size_t)j * nE + e);
-      const int r = ld(m.e_rev, (size_t)j * nE + e);
       const R wj = ld(m.e_w, (size_t)j * nE + e);
-      const R wr = ld(m.e_w, (size_t)r * nE + nb);
+      const R wr = ld(m.e_wrev, (size_t)j * nE + e);
       pe_ad = pe_ad + R(0.5) * (((wj * ld(bs.u, nb)) * ld(bs.he, nb)) * Te);
-      const R Tn = ad_tu(in, B, nb, b);
+      const R Tn = in.tu[(size_t)nb * B + b];
       const R wpv = R(0.5) * (ld(bs.pe, nb) + pee);
       he_ad = he_ad + ((wr * ue) * wpv) * Tn;
       pe_ad = pe_ad + R(0.5) * (((wr * ue) * hee) * Tn);
@@ -483,7 +486,7 @@ __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A
     }
     const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
     const R dv = ld(m.e_dv, e);
-    const R fa = ad_th(in, B, c2, b) / ld(m.c_area, c2) - ad_th(in, B, c1, b) / ld(m.c_area, c1);
+    const R fa = in.th[(size_t)c2 * B + b] - in.th[(size_t)c1 * B + b];
     he_ad = he_ad + (ue * dv) * fa;
     ud = ud + (dv * hee) * fa;
     if (ph.drag) {
@@ -515,7 +518,7 @@ __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A
 // del4 adjoint, first half (:588-634): delsq_vorticity/delsq_circulation adjoint on vertices
 // and delsq_divergence adjoint on cells.
 template <typename R, typename A>
-__global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R, A> in, AdWork<R> w) {
+__global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R> in, AdWork<R> w) {
   const int nV = m.nV, nC = m.nC;
   const long long tv = (long long)nV * B;
   MPSW_GRID_LOOP(t, tv + (long long)nC * B) {
@@ -526,7 +529,7 @@ __global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R, A> in, AdW
       for (int k = 0; k < VDEG; k++) {
         const int e = ld(m.v_es, (size_t)k * nV + v);
         const R sg = R(m.v_esg[(size_t)k * nV + v]);
-        const R ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-ad_tu(in, B, e, b));
+        const R ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-in.tu[(size_t)e * B + b]);
         acc = acc + (-sg) * (ud4 / ld(m.e_dv, e));
       }
       w.dc_ad[(size_t)v * B + b] = acc * (R(1) / ld(m.v_area, v));
@@ -538,7 +541,7 @@ __global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R, A> in, AdW
       for (int k = 0; k < n; k++) {
         const int e = ld(m.c_es, (size_t)k * nC + c);
         const R sg = R(m.c_esg[(size_t)k * nC + c]);
-        const R ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-ad_tu(in, B, e, b));
+        const R ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-in.tu[(size_t)e * B + b]);
         acc = acc + (-sg) * (ud4 / ld(m.e_dc, e));
       }
       w.dd_ad[(size_t)c * B + b] = acc * (R(1) / ld(m.c_area, c));
@@ -566,7 +569,7 @@ __global__ void k_ad_del4_e(MeshDev<R> m, int B, AdWork<R> w) {
 // adjoint (:696-699), drag ke terms, del2/del4 divergence adjoints, h_edge adjoint (:358-369),
 // then the 1/areaCell scalings of ke_ad and divergence_ad (:306-326).
 template <typename R, typename A>
-__global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A> in, AdSeeds<R> sd,
+__global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                           AdWork<R> w) {
   const int nC = m.nC;
   MPSW_GRID_LOOP(t, (long long)nC * B) {
@@ -580,7 +583,7 @@ __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A
       const int e = ld(m.c_es, (size_t)k * nC + c);
       const R sg = R(m.c_esg[(size_t)k * nC + c]);
       const size_t oe = (size_t)e * B + b;
-      const R Te = ad_tu(in, B, e, b);
+      const R Te = in.tu[(size_t)e * B + b];
       const R dce = ld(m.e_dc, e);
       pc_ad = pc_ad + (-sg) * (w.gpn_ad[oe] / dce);
       ke_ad = ke_ad + sg * (Te / dce);
@@ -610,7 +613,7 @@ __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A
 // gradPVt -> pv_vertex (:254-262), del2/del4 vorticity adjoints, pv_vertex -> h_vertex and
 // vorticity (:268-284), vorticity -> circulation (:343-349).
 template <typename R, typename A>
-__global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R, A> in,
+__global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in,
                             AdSeeds<R> sd, AdWork<R> w) {
   const int nV = m.nV;
   MPSW_GRID_LOOP(t, (long long)nV * B) {
@@ -635,7 +638,7 @@ __global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R,
       const size_t oe = (size_t)e * B + b;
       pvv_ad = pvv_ad + sg * (w.gpt_ad[oe] / dve);
       if (ph.visc2 > R(0)) {
-        const R ud2 = (ld(m.e_sc2, e) * ph.visc2) * ad_tu(in, B, e, b);
+        const R ud2 = (ld(m.e_sc2, e) * ph.visc2) * in.tu[(size_t)e * B + b];
         vort_ad = vort_ad + (-sg) * (ud2 / dve);
       }
       if (ph.visc4 > R(0)) vort_ad = vort_ad + (-sg) * (w.du_ad[oe] / dve);
@@ -653,19 +656,23 @@ __global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R,
 }
 
 template <typename R, typename A>
-__device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, size_t o, R pad) {
-  R *pp = is_edge ? out.pad_u : out.pad_h;
-  if (pp) pp[o] = pad;
+__device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, size_t o, R pad, R area) {
   A *acc = is_edge ? out.acc_u : out.acc_h;
-  if (out.mode == AD_SET) {
-    if (acc) acc[o] = A(pad);
-  } else if (out.mode == AD_ADD) {
-    if (acc) acc[o] = acc[o] + A(pad);
-  } else {
-    const A *x2 = is_edge ? out.x2u : out.x2h;
+  const A *x2 = is_edge ? out.x2u : out.x2h;
+  R *tn = is_edge ? out.tu_next : out.th_next;
+  const A wn = is_edge ? out.wu : out.wh, cn = is_edge ? out.cu : out.ch;
+  A next;
+  if (out.mode == AD_FINAL) {
     A *dst = is_edge ? out.dst_u : out.dst_h;
-    dst[o] = (acc[o] + x2[o]) + A(pad);
+    const A d = (acc[o] + x2[o]) + A(pad);
+    dst[o] = d;
+    next = wn * d;
+  } else {
+    if (out.mode == AD_SET) acc[o] = A(pad);
+    else acc[o] = acc[o] + A(pad);
+    next = (x2 ? wn * x2[o] : A(0)) + cn * A(pad);
   }
+  if (tn) tn[o] = is_edge ? R(next) : R(next / A(area));
 }
 
 // Final stage of the adjoint: h_vertex -> h (:286-289) on cells, and on edges the transposed
@@ -682,7 +689,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
       R ph_ = w.hd[(size_t)c * B + b];
       for (int k = 0; k < n; k++)
         ph_ = ph_ + ld(m.c_vk, (size_t)k * nC + c) * w.hv_ad[(size_t)ld(m.c_vs, (size_t)k * nC + c) * B + b];
-      ad_emit(out, 0, (size_t)c * B + b, ph_);
+      ad_emit(out, 0, (size_t)c * B + b, ph_, ld(m.c_area, c));
     } else {
       const long long t2 = t - tc;
       const int e = (int)(t2 / B), b = (int)(t2 - (long long)e * B);
@@ -690,8 +697,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
       R pu = w.ud[(size_t)e * B + b];
       for (int j = 0; j < n; j++) {
         const int nb = ld(m.e_eoe, (size_t)j * nE + e);
-        const int r = ld(m.e_rev, (size_t)j * nE + e);
-        pu = pu + ld(m.e_w, (size_t)r * nE + nb) * w.v_ad[(size_t)nb * B + b];
+        pu = pu + ld(m.e_wrev, (size_t)j * nE + e) * w.v_ad[(size_t)nb * B + b];
       }
       const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
       const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
@@ -702,7 +708,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
       pu = pu + dv * w.div_ad[(size_t)c1 * B + b];
       pu = pu + dc * w.circ_ad[(size_t)v2 * B + b];
       pu = pu - dc * w.circ_ad[(size_t)v1 * B + b];
-      ad_emit(out, 1, (size_t)e * B + b, pu);
+      ad_emit(out, 1, (size_t)e * B + b, pu, R(1));
     }
   }
 }

@@ -80,7 +80,7 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
-                            const AdIn<R, A> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
+                            const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
                             const AdOut<R, A> &out, cudaStream_t s) {
   g_launches++;
   k_ad_edge<R, A><<<grid_for((long long)m.nE * B), kThreads, 0, s>>>(m, B, bs, ph, in, sd, w);
@@ -99,7 +99,7 @@ void Launch<R, A>::ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
-                           const AdIn<R, A> &in, const AdWork<R> &w, const AdOut<R, A> &out,
+                           const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out,
                            cudaStream_t s) {
   const AdSeeds<R> sd{};
   g_launches++;
@@ -109,6 +109,13 @@ void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> 
     case 2: k_ad_vertex<R, A><<<grid_for((long long)m.nV * B), kThreads, 0, s>>>(m, B, bs, ph, in, sd, w); break;
     default: k_ad_final<R, A><<<grid_for((long long)(m.nC + m.nE) * B), kThreads, 0, s>>>(m, B, bs, w, out); break;
   }
+}
+template <typename R, typename A>
+void Launch<R, A>::ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,
+                            const R *seed_th, A wu, A wh, R *tu, R *th, cudaStream_t s) {
+  g_launches++;
+  k_ad_tinit<R, A><<<grid_for((long long)(m.nE + m.nC) * B), kThreads, 0, s>>>(m, B, x2u, x2h, seed_tu,
+                                                                             seed_th, wu, wh, tu, th);
 }
 template <typename R, typename A>
 void Launch<R, A>::recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea,

@@ -38,11 +38,13 @@ struct Launch {
                            cudaStream_t s);
   // adjoint of one stage, B members
   static void ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
-                       const AdIn<R, A> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
+                       const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
                        const AdOut<R, A> &out, cudaStream_t s);
   // one kernel of ad_stage (0 edge, 1 cell, 2 vertex, 3 final), for timing
   static void ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
-                      const AdIn<R, A> &in, const AdWork<R> &w, const AdOut<R, A> &out, cudaStream_t s);
+                      const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out, cudaStream_t s);
+  static void ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,
+                       const R *seed_th, A wu, A wh, R *tu, R *th, cudaStream_t s);
   static void recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea, A *u_ad,
                         cudaStream_t s);
   // boundary

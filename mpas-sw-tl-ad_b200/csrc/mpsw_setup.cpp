@@ -391,6 +391,7 @@ std::string build_mesh(const RefMesh &m, const RefGeometry &g, int sfc, BuiltMes
   o->e_eoe.assign((size_t)MAXE2 * nE, 0);
   o->e_rev.assign((size_t)MAXE2 * nE, 0);
   o->e_w.assign((size_t)MAXE2 * nE, 0.0);
+  o->e_wrev.assign((size_t)MAXE2 * nE, 0.0);
   o->e_dc.assign(nE, 0.0); o->e_dv.assign(nE, 0.0); o->e_sc2.assign(nE, 1.0); o->e_sc4.assign(nE, 1.0);
   o->e_usrc.assign(nE, 0.0);
   for (int e = 0; e < nE; e++) {
@@ -422,6 +423,7 @@ std::string build_mesh(const RefMesh &m, const RefGeometry &g, int sfc, BuiltMes
       o->e_eoe[(size_t)j * nE + ei] = pe[nb];
       o->e_rev[(size_t)j * nE + ei] = r;
       o->e_w[(size_t)j * nE + ei] = rd(m.weightsOnEdge, mE2, j + 1, e + 1);
+      o->e_wrev[(size_t)j * nE + ei] = rd(m.weightsOnEdge, mE2, r + 1, nb + 1);
     }
     o->e_dc[ei] = m.dcEdge[e];
     o->e_dv[ei] = m.dvEdge[e];

@@ -41,7 +41,7 @@ struct BuiltMesh {
   std::vector<signed char> c_esg, v_esg;
   std::vector<double> c_vk, c_area, c_hs, c_coef, c_trig;
   std::vector<int> e_c1, e_c2, e_v1, e_v2, e_va, e_vb, e_slot1, e_slot2, e_n, e_eoe, e_rev;
-  std::vector<double> e_w, e_dc, e_dv, e_sc2, e_sc4, e_usrc;
+  std::vector<double> e_w, e_wrev, e_dc, e_dv, e_sc2, e_sc4, e_usrc;
   std::vector<int> v_es, v_c, v_e;
   std::vector<double> v_k, v_area, v_f;
 };

@@ -56,6 +56,7 @@ template <typename R>
 MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   Window::Members &M = E.win.ms[prec];
   if (M.bufs && M.B >= B) return (MemberBufs<R> *)M.bufs;
+  E.graphs_free();  // captured steps point at the buffers about to be replaced
   free_members<R>(M);
   auto *mb = new MemberBufs<R>();
   const size_t C = (size_t)E.nC * B, Ed = (size_t)E.nE * B, V = (size_t)E.nV * B;
@@ -133,8 +134,58 @@ void rk_coeffs(double dt, double w[4], double c[4]) {
 
 }  // namespace
 
+void Engine::graphs_free() {
+  for (auto &g : graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  graphs.clear();
+}
+
+GraphKey Engine::graph_key(int kind, int prec, int B, const void *p1, const void *p2) const {
+  const Phys<double> ph = phys();
+  GraphKey k;
+  k.kind = kind; k.prec = prec; k.B = B; k.p1 = p1; k.p2 = p2;
+  k.dt = ph.dt; k.apvm = ph.apvm; k.visc2 = ph.visc2; k.visc4 = ph.visc4;
+  k.flags = ph.wind | (ph.drag << 1) | (ph.tc1 << 2) | (ph.sphere << 3);
+  return k;
+}
+
+// Run `body` (kernel launches on the engine stream, no allocation, no synchronisation) as a
+// CUDA graph: captured on first use for this key, replayed afterwards.  MPSW_GRAPHS=0 runs it
+// eagerly instead.
+template <typename F>
+void Engine::run_graph(const GraphKey &k, F &&body) {
+  static const bool enabled = !(getenv("MPSW_GRAPHS") && atoi(getenv("MPSW_GRAPHS")) == 0);
+  if (!enabled) {
+    body();
+    return;
+  }
+  for (auto &g : graphs)
+    if (g.key == k) {
+      cuda_check(cudaGraphLaunch(g.exec, stream), "cudaGraphLaunch");
+      return;
+    }
+  cudaGraph_t graph = nullptr;
+  cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
+  GraphEntry e;
+  e.key = k;
+  const cudaError_t st = cudaGraphInstantiate(&e.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(st, "cudaGraphInstantiate");
+  graphs.push_back(e);
+  cuda_check(cudaGraphLaunch(e.exec, stream), "cudaGraphLaunch");
+}
+
 void Engine::window_free() {
   Window &W = win;
+  graphs_free();
   free_members<double>(W.ms[0]);
   free_members<float>(W.ms[1]);
   window_free_trajectory();
@@ -142,6 +193,7 @@ void Engine::window_free() {
 
 void Engine::window_free_trajectory() {
   Window &W = win;
+  graphs_free();
   for (double *p : W.ck_u) cudaFree(p);
   for (double *p : W.ck_h) cudaFree(p);
   W.ck_u.clear();
@@ -268,7 +320,7 @@ void Engine::window_trajectory(cudaStream_t s) {
       cuda_check(cudaMemcpyAsync(W.ck_u[n / W.every], W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "ckpt");
       cuda_check(cudaMemcpyAsync(W.ck_h[n / W.every], W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "ckpt");
     }
-    traj_step(*this, true, 0, [](int) {});
+    run_graph(graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(*this, true, 0, [](int) {}); });
   }
   cuda_check(cudaMemcpyAsync(W.fin_u, W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "final");
   cuda_check(cudaMemcpyAsync(W.fin_h, W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "final");
@@ -287,7 +339,7 @@ static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
   rk_coeffs(ph64.dt, w, c);
   cuda_check(cudaMemcpyAsync(W.x_u, W.ck_u[0], sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
   cuda_check(cudaMemcpyAsync(W.x_h, W.ck_h[0], sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
-  for (int n = 0; n < W.nsteps; n++) {
+  auto step = [&]() {
     traj_step(E, true, prec, [&](int k) {
       const Base<R> bs = base_for<R>(W, k);
       const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
@@ -315,7 +367,9 @@ static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
       if (ph64.visc4 > 0) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
       Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, E.stream);
     });
-  }
+  };
+  const GraphKey key = E.graph_key(2, prec, B, du, dh);
+  for (int n = 0; n < W.nsteps; n++) E.run_graph(key, step);
   cuda_check(cudaGetLastError(), "window_tl");
 }
 
@@ -329,6 +383,11 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
   AdSeeds<R> none{};
+  Window::Members &M = W.ms[prec];
+  const double wu4 = ph64.tc1 ? 0.0 : w[3];
+  // tendency adjoint of the last stage of the last step; later steps get theirs from the
+  // final stage of the step after them
+  Launch<R, double>::ad_tinit(m, B, au, ah, nullptr, nullptr, wu4, w[3], mb->pad_u[0], mb->pad_h[0], E.stream);
   for (int s = W.nckpt - 1; s >= 0; s--) {
     const int first = s * W.every, len = std::min(W.every, W.nsteps - first);
     // replay the segment, keeping the start state of every step
@@ -337,26 +396,34 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
     for (int j = 0; j < len; j++) {
       cuda_check(cudaMemcpyAsync(W.seg_u + (size_t)j * E.nE, W.x_u, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "seg");
       cuda_check(cudaMemcpyAsync(W.seg_h + (size_t)j * E.nC, W.x_h, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "seg");
-      if (j + 1 < len) traj_step(E, true, 0, [](int) {});
+      if (j + 1 < len) E.run_graph(E.graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(E, true, 0, [](int) {}); });
     }
     for (int j = len - 1; j >= 0; j--) {
       cuda_check(cudaMemcpyAsync(W.x_u, W.seg_u + (size_t)j * E.nE, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
       cuda_check(cudaMemcpyAsync(W.x_h, W.seg_h + (size_t)j * E.nC, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
+      E.run_graph(E.graph_key(3, prec, B, au, ah), [&]() {
       // forward sweep of this step, keeping the four stages' linearisation points
       traj_step(E, false, prec, [](int) {});
       for (int k = 3; k >= 0; k--) {
-        AdIn<R, double> in{};
-        in.x2u = au; in.x2h = ah; in.w = w[k]; in.c = c[k]; in.tc1 = ph.tc1;
-        in.pnu = k == 3 ? nullptr : mb->pad_u[(k + 1) & 1];
-        in.pnh = k == 3 ? nullptr : mb->pad_h[(k + 1) & 1];
+        AdIn<R> in{mb->pad_u[(3 - k) & 1], mb->pad_h[(3 - k) & 1]};
         AdOut<R, double> out{};
-        out.pad_u = k == 0 ? nullptr : mb->pad_u[k & 1];
-        out.pad_h = k == 0 ? nullptr : mb->pad_h[k & 1];
-        out.acc_u = W.ms[prec].acc_u; out.acc_h = W.ms[prec].acc_h;
-        out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
+        out.acc_u = M.acc_u; out.acc_h = M.acc_h;
         out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
+        out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
+        out.tu_next = mb->pad_u[(4 - k) & 1];
+        out.th_next = mb->pad_h[(4 - k) & 1];
+        if (k > 0) {
+          out.wu = ph64.tc1 ? 0.0 : w[k - 1];
+          out.cu = ph64.tc1 ? 0.0 : c[k - 1];
+          out.wh = w[k - 1];
+          out.ch = c[k - 1];
+        } else {  // stage 4 of the preceding step: tend_ad = w4 * (this step's input adjoint)
+          out.wu = wu4;
+          out.wh = w[3];
+        }
         Launch<R, double>::ad_stage(m, B, base_for<R>(W, k), ph, in, none, mb->w, out, E.stream);
       }
+      });
     }
   }
   cuda_check(cudaGetLastError(), "window_ad");
@@ -460,12 +527,12 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
   rk_coeffs(ph64.dt, w, c);
   RK<R, double> rku{W.ms[prec].acc_u, W.ms[prec].acc_u, W.ms[prec].acc_u, mb->pu[1], c[1], w[1], R(0), 0};
   RK<R, double> rkh{W.ms[prec].acc_h, W.ms[prec].acc_h, W.ms[prec].acc_h, mb->ph[1], c[1], w[1], R(0), 0};
-  AdIn<R, double> in{};
-  in.x2u = W.ms[prec].acc_u; in.x2h = W.ms[prec].acc_h; in.pnu = mb->pad_u[0]; in.pnh = mb->pad_h[0];
-  in.w = w[1]; in.c = c[1];
+  AdIn<R> in{mb->pad_u[0], mb->pad_h[0]};
   AdOut<R, double> out{};
-  out.pad_u = mb->pad_u[1]; out.pad_h = mb->pad_h[1];
   out.acc_u = W.ms[prec].acc_u; out.acc_h = W.ms[prec].acc_h; out.mode = AD_ADD;
+  out.x2u = W.ms[prec].acc_u; out.x2h = W.ms[prec].acc_h;
+  out.tu_next = mb->pad_u[1]; out.th_next = mb->pad_h[1];
+  out.wu = w[1]; out.cu = c[1]; out.wh = w[1]; out.ch = c[1];
   auto launch = [&]() {
     using LR = Launch<R, double>;
     switch (which) {

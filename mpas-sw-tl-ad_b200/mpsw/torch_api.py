@@ -86,6 +86,7 @@ class Window:
     def __init__(self, engine: Engine, nsteps: int, ckpt_every: int = 16):
         self.e = engine
         self.nsteps = nsteps
+        engine.module.sync()  # pending host-side edits of the module's state first
         engine.h.call('mpsw_window_init', int(nsteps), int(ckpt_every), _stream())
 
     def final_state(self):
