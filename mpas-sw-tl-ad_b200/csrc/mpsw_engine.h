@@ -71,6 +71,7 @@ struct GraphKey {
 struct GraphEntry {
   GraphKey key;
   cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;  // kernel launches recorded in the graph
 };
 
 struct Engine {

@@ -162,9 +162,11 @@ void Engine::run_graph(const GraphKey &k, F &&body) {
   for (auto &g : graphs)
     if (g.key == k) {
       cuda_check(cudaGraphLaunch(g.exec, stream), "cudaGraphLaunch");
+      g_launches += g.kernels;
       return;
     }
   cudaGraph_t graph = nullptr;
+  const long long before = g_launches;
   cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
   try {
     body();
@@ -176,6 +178,7 @@ void Engine::run_graph(const GraphKey &k, F &&body) {
   cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
   GraphEntry e;
   e.key = k;
+  e.kernels = g_launches - before;  // counted once here, then once per replay
   const cudaError_t st = cudaGraphInstantiate(&e.exec, graph, 0);
   cudaGraphDestroy(graph);
   cuda_check(st, "cudaGraphInstantiate");
