@@ -106,6 +106,25 @@ int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah,
 /* Final nonlinear state of the window (device buffers, internal order). */
 int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream);
 
+/* ---- tendencies without device allocation ------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory when they
+ * need the model (a host system that reserves all GPU memory for its own pool at start-up, or
+ * code that must not synchronise the device the way cudaFree does): the tendencies tend_u,
+ * tend_h of the state (u, hh), exactly as mpsw_compute_tend computes them, with the
+ * intermediate diagnostics kept in a fixed 16 MiB array inside the library's device image
+ * (held by every GPU that loads the library until the process exits).  All buffers are device
+ * memory in the engine's internal order (see mpsw_to_internal): u and tend_u nEdges doubles,
+ * hh and tend_h nCells doubles.  Needs sw_mpas_init_block to have put the mesh on the device;
+ * the mesh must need at most 2,097,152 doubles of scratch, 3*nVertices + 3*nCells +
+ * 2*nEdges (plus nEdges + nVertices + nCells with del4 viscosity), i.e. up to about 140,000
+ * cells (100,000 with del4) on a quasi-uniform mesh; larger meshes are refused with
+ * MPSW_ERR_UNSUPPORTED.  On success the call allocates
+ * nothing; the first call on each device looks up the array's address (make that first call
+ * before any stream capture).  Every call on a device shares the array, so calls whose work
+ * overlaps on the GPU (other streams, other threads, other handles) race; order them. */
+int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const double *hh, double *tend_u,
+                              double *tend_h, void *stream);
+
 /* ---- measurement ----------------------------------------------------------------------- */
 /* Number of kernels the library has launched in this process (all handles). */
 long long mpsw_launch_count(void);

@@ -172,6 +172,7 @@ long long Engine::dim_of(const std::string &sym) const {
 
 Engine::Engine() {
   for (const auto &s : kScalars) scal[s.name] = s.def;
+  refresh_phys();
   for (const auto &s : specs()) {
     Var v;
     v.name = s.name;
@@ -522,8 +523,10 @@ void Engine::mark_recon(int g) {
   for (int i = 0; i < 5; i++) mark_written(var((std::string(kDiagNames[i]) + sfx).c_str()), g != 2);
 }
 
-Phys<double> Engine::phys() const {
-  Phys<double> p{};
+Phys<double> Engine::phys() const { return phys_cache; }
+
+void Engine::refresh_phys() {
+  Phys<double> &p = phys_cache;
   p.dt = sc("config_dt");
   p.apvm = sc("config_apvm_upwinding");
   p.visc2 = sc("config_h_mom_eddy_visc2");
@@ -532,7 +535,6 @@ Phys<double> Engine::phys() const {
   p.drag = sc("config_bottom_drag") != 0.0;
   p.tc1 = (int)sc("config_test_case") == 1;
   p.sphere = sc("on_a_sphere") != 0.0;
-  return p;
 }
 
 // ---- stage building blocks ---------------------------------------------------------------
@@ -926,6 +928,7 @@ int mpsw_set_scalar(mpsw_handle *h, const char *name, double value) {
       if (n == s.name && s.readonly) throw mpsw::EngineError(MPSW_ERR_ARG, "cannot assign a parameter: " + n);
     if (n == "on_a_sphere" || n == "config_h_scalewithmesh") e.mesh_dirty = true;
     e.scal[n] = value;
+    e.refresh_phys();
   });
 }
 

@@ -102,6 +102,8 @@ struct Engine {
   AdWork<double> adw{};
   double *tu_[2] = {}, *th_[2] = {}, *xacc_u = nullptr, *xacc_h = nullptr;
   int pending_diag = 0;  // 1: diagnostics of the level-1 state owed, 2: and their tangents
+  Phys<double> phys_cache{};  // physics scalars, refreshed whenever a scalar is assigned
+  void refresh_phys();
   Window win;
 
   Engine();

@@ -50,6 +50,7 @@ SIGNATURES = {
     'mpsw_state_from_device': (_c_int, [_vp, _vp, _vp, _vp]),
     'mpsw_state_to_device': (_c_int, [_vp, _vp, _vp, _vp]),
     'mpsw_launch_count': (_ll, []),
+    'mpsw_compute_tend_noalloc': (_c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     'mpsw_time_kernel': (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_c_double)]),
 }
 
