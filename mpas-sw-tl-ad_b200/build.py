@@ -33,7 +33,7 @@ UNITS = [
     ('mpsw_noalloc.cu', ['--fmad=false']),
     ('mpsw_setup.cpp', ['--fmad=false', '-x', 'cu']),
 ]
-HEADERS = ['mpsw_internal.h', 'mpsw_kernels.cuh', 'mpsw_launch.h', 'mpsw_launch.cuh',
+HEADERS = ['mpsw_internal.h', 'mpsw_kernels.cuh', 'mpsw_launch.h', 'mpsw_launch.cuh', 'mpsw_members.cuh',
            'mpsw_setup.h', 'mpsw_engine.h']
 
 

@@ -2,8 +2,13 @@
 // per precision, which also instantiates them).
 #pragma once
 
+#include <cstdint>
+#include <cstdlib>
+#include <initializer_list>
+
 #include "mpsw_kernels.cuh"
 #include "mpsw_launch.h"
+#include "mpsw_members.cuh"
 
 namespace mpsw {
 
@@ -27,6 +32,37 @@ inline LaunchCfg launch_cfg(long long total) {
 // every kernel launch of the engine goes through one of these launchers and is counted here
 extern long long g_launches;
 
+// Members per thread of a member kernel: 16 bytes of R per vector load (4 floats, 2 doubles),
+// reduced while B is not a multiple of it or a buffer is not aligned to V elements of the wider
+// of R and A.  MPSW_VEC=1|2|4 overrides the starting width.
+template <typename R, typename A>
+inline int vec_width(int B, std::initializer_list<const void *> ptrs) {
+  static const int forced = [] {
+    const char *e = std::getenv("MPSW_VEC");
+    const int v = e ? std::atoi(e) : 0;
+    return (v == 1 || v == 2 || v == 4) ? v : 0;
+  }();
+  int v = forced ? forced : (int)(16 / sizeof(R));
+  const size_t wide = sizeof(R) > sizeof(A) ? sizeof(R) : sizeof(A);
+  for (; v > 1; v >>= 1) {
+    if (B % v) continue;
+    bool ok = true;
+    for (const void *p : ptrs)
+      if (p && ((uintptr_t)p % (v * wide))) ok = false;
+    if (ok) break;
+  }
+  return v;
+}
+
+// run the statement with the compile-time member width VV equal to the runtime width v
+#define MPSW_VDISPATCH(v, ...)                            \
+  switch (v) {                                            \
+    case 4: { constexpr int VV = 4; __VA_ARGS__; } break;  \
+    case 2: { constexpr int VV = 2; __VA_ARGS__; } break;  \
+    default: { constexpr int VV = 1; __VA_ARGS__; } break; \
+  }
+#define LCFGV(n, B, v) LCFG((long long)(n) * ((B) / (v)))
+
 template <typename R, typename A>
 void Launch<R, A>::fwd_vertex(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                               cudaStream_t s) {
@@ -49,7 +85,8 @@ template <typename R, typename A>
 void Launch<R, A>::del4_vc(const MeshDev<R> &m, int B, const R *dsq_u, R *dsq_vort, R *dsq_div,
                            cudaStream_t s) {
   g_launches++;
-  k_del4_vc<R><<<LCFG((long long)(m.nV + m.nC) * B), 0, s>>>(m, B, dsq_u, dsq_vort, dsq_div);
+  const int v = vec_width<R, A>(B, {dsq_u, dsq_vort, dsq_div});
+  MPSW_VDISPATCH(v, (k_del4_vc<R, VV><<<LCFGV(m.nV + m.nC, B, VV), 0, s>>>(m, B, dsq_u, dsq_vort, dsq_div)));
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
@@ -72,65 +109,87 @@ template <typename R, typename A>
 void Launch<R, A>::tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                              const Diag<R> &d, cudaStream_t s) {
   g_launches++;
-  k_tl_vertex<R><<<LCFG((long long)m.nV * B), 0, s>>>(m, B, bs, ut, ht, d);
+  const int v = vec_width<R, A>(B, {ut, ht, d.circ, d.vort, d.hv, d.pvv});
+  MPSW_VDISPATCH(v, (k_tl_vertex<R, VV><<<LCFGV(m.nV, B, VV), 0, s>>>(m, B, bs, ut, ht, d)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                            const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
-  k_tl_cell<R, A><<<LCFG((long long)m.nC * B), 0, s>>>(m, B, bs, ut, ht, d, rk, tend_h);
+  const int v = vec_width<R, A>(B, {ut, ht, d.div, d.ke, d.pc, d.vc, d.pvv, d.vort, tend_h, rk.x0, rk.acc_in,
+                                    rk.acc_out, rk.next});
+  MPSW_VDISPATCH(v, (k_tl_cell<R, A, VV><<<LCFGV(m.nC, B, VV), 0, s>>>(m, B, bs, ut, ht, d, rk, tend_h)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                                 const Diag<R> &d, const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
-  k_tl_edge_diag<R><<<LCFG((long long)m.nE * B), 0, s>>>(m, B, bs, ut, ht, d, ph);
+  const int v = vec_width<R, A>(B, {ut, ht, d.pvv, d.pc, d.div, d.vort, d.pe, d.he, d.v, d.gpt, d.gpn, d.dsq_u});
+  MPSW_VDISPATCH(v, (k_tl_edge_diag<R, VV><<<LCFGV(m.nE, B, VV), 0, s>>>(m, B, bs, ut, ht, d, ph)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                                 const Diag<R> &d, const Phys<R> &ph, const RK<R, A> &rk, R *tend_u,
                                 cudaStream_t s) {
   g_launches++;
-  k_tl_edge_tend<R, A><<<LCFG((long long)m.nE * B), 0, s>>>(m, B, bs, ut, ht, d, ph, rk, tend_u);
+  const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
+                                    rk.x0, rk.acc_in, rk.acc_out, rk.next});
+  MPSW_VDISPATCH(v, (k_tl_edge_tend<R, A, VV><<<LCFGV(m.nE, B, VV), 0, s>>>(m, B, bs, ut, ht, d, ph, rk, tend_u)));
 }
+// members per thread of one adjoint stage: every buffer the five kernels touch
+template <typename R, typename A>
+static int ad_width(int B, const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out) {
+  return vec_width<R, A>(B, {in.tu, in.th, w.pe_ad, w.he_ad, w.ud, w.gpn_ad, w.gpt_ad, w.v_ad, w.du_ad, w.pc_ad,
+                             w.ke_ad, w.div_ad, w.hd, w.dd_ad, w.hv_ad, w.circ_ad, w.dc_ad, out.acc_u, out.acc_h,
+                             out.x2u, out.x2h, out.dst_u, out.dst_h, out.tu_next, out.th_next});
+}
+
+template <typename R, typename A, int V>
+static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
+                      const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w, const AdOut<R, A> &out,
+                      cudaStream_t s) {
+  g_launches++;
+  switch (which) {
+    case 0: k_ad_edge<R, A, V><<<LCFGV(m.nE, B, V), 0, s>>>(m, B, bs, ph, in, sd, w); break;
+    case 1: k_ad_cell<R, A, V><<<LCFGV(m.nC, B, V), 0, s>>>(m, B, bs, ph, in, sd, w); break;
+    case 2: k_ad_vertex<R, A, V><<<LCFGV(m.nV, B, V), 0, s>>>(m, B, bs, ph, in, sd, w); break;
+    case 3: k_ad_final<R, A, V><<<LCFGV(m.nC + m.nE, B, V), 0, s>>>(m, B, bs, w, out); break;
+    case 4: k_ad_del4_vc<R, V><<<LCFGV(m.nV + m.nC, B, V), 0, s>>>(m, B, ph, in, w); break;
+    default: k_ad_del4_e<R, V><<<LCFGV(m.nE, B, V), 0, s>>>(m, B, w); break;
+  }
+}
+
 template <typename R, typename A>
 void Launch<R, A>::ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                             const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
                             const AdOut<R, A> &out, cudaStream_t s) {
-  g_launches++;
-  k_ad_edge<R, A><<<LCFG((long long)m.nE * B), 0, s>>>(m, B, bs, ph, in, sd, w);
-  if (ph.visc4 > R(0)) {
-    g_launches++;
-    k_ad_del4_vc<R, A><<<LCFG((long long)(m.nV + m.nC) * B), 0, s>>>(m, B, ph, in, w);
-    g_launches++;
-    k_ad_del4_e<R><<<LCFG((long long)m.nE * B), 0, s>>>(m, B, w);
-  }
-  g_launches++;
-  k_ad_cell<R, A><<<LCFG((long long)m.nC * B), 0, s>>>(m, B, bs, ph, in, sd, w);
-  g_launches++;
-  k_ad_vertex<R, A><<<LCFG((long long)m.nV * B), 0, s>>>(m, B, bs, ph, in, sd, w);
-  g_launches++;
-  k_ad_final<R, A><<<LCFG((long long)(m.nC + m.nE) * B), 0, s>>>(m, B, bs, w, out);
+  const int v = ad_width<R, A>(B, in, w, out);
+  MPSW_VDISPATCH(v, {
+    ad_launch<R, A, VV>(0, m, B, bs, ph, in, sd, w, out, s);
+    if (ph.visc4 > R(0)) {
+      ad_launch<R, A, VV>(4, m, B, bs, ph, in, sd, w, out, s);
+      ad_launch<R, A, VV>(5, m, B, bs, ph, in, sd, w, out, s);
+    }
+    ad_launch<R, A, VV>(1, m, B, bs, ph, in, sd, w, out, s);
+    ad_launch<R, A, VV>(2, m, B, bs, ph, in, sd, w, out, s);
+    ad_launch<R, A, VV>(3, m, B, bs, ph, in, sd, w, out, s);
+  });
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                            const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out,
                            cudaStream_t s) {
   const AdSeeds<R> sd{};
-  g_launches++;
-  switch (which) {
-    case 0: k_ad_edge<R, A><<<LCFG((long long)m.nE * B), 0, s>>>(m, B, bs, ph, in, sd, w); break;
-    case 1: k_ad_cell<R, A><<<LCFG((long long)m.nC * B), 0, s>>>(m, B, bs, ph, in, sd, w); break;
-    case 2: k_ad_vertex<R, A><<<LCFG((long long)m.nV * B), 0, s>>>(m, B, bs, ph, in, sd, w); break;
-    default: k_ad_final<R, A><<<LCFG((long long)(m.nC + m.nE) * B), 0, s>>>(m, B, bs, w, out); break;
-  }
+  const int v = ad_width<R, A>(B, in, w, out);
+  MPSW_VDISPATCH(v, (ad_launch<R, A, VV>(which < 0 || which > 3 ? 3 : which, m, B, bs, ph, in, sd, w, out, s)));
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,
                             const R *seed_th, A wu, A wh, R *tu, R *th, cudaStream_t s) {
   g_launches++;
-  k_ad_tinit<R, A><<<LCFG((long long)(m.nE + m.nC) * B), 0, s>>>(m, B, x2u, x2h, seed_tu,
-                                                                             seed_th, wu, wh, tu, th);
+  const int v = vec_width<R, A>(B, {x2u, x2h, tu, th});
+  MPSW_VDISPATCH(v, (k_ad_tinit<R, A, VV><<<LCFGV(m.nE + m.nC, B, VV), 0, s>>>(m, B, x2u, x2h, seed_tu, seed_th,
+                                                                                wu, wh, tu, th)));
 }
 template <typename R, typename A>
 void Launch<R, A>::recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea,

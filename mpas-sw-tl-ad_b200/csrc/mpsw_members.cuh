@@ -1,0 +1,648 @@
+// Member kernels: tangent linear and adjoint of the RK4 stages for B members about one stored
+// linearisation point, and the del4 intermediates.
+//
+// Member arrays are [n][B]; each thread holds V consecutive members of one entity (Mv<R,V>)
+// and moves them with vector loads, so the connectivity, weights and linearisation-point
+// values of a neighbour are loaded once for V independent accumulation chains.  Every
+// member's arithmetic is the scalar expression of the reference, element by element, so V
+// does not change a single rounding (V = 1 is the single-member module path).
+#pragma once
+
+#include "mpsw_kernels.cuh"
+
+namespace mpsw {
+
+// ---- V members of one entity -------------------------------------------------------------
+template <typename R, int V>
+struct alignas(sizeof(R) * V) Mv {
+  R x[V];
+};
+
+#define MPSW_MV_OP(op)                                                                            \
+  template <typename R, int V>                                                                  \
+  __device__ __forceinline__ Mv<R, V> operator op(const Mv<R, V> &a, const Mv<R, V> &b) {       \
+    Mv<R, V> r;                                                                                 \
+    _Pragma("unroll") for (int i = 0; i < V; i++) r.x[i] = a.x[i] op b.x[i];                    \
+    return r;                                                                                   \
+  }                                                                                             \
+  template <typename R, int V>                                                                  \
+  __device__ __forceinline__ Mv<R, V> operator op(R a, const Mv<R, V> &b) {                     \
+    Mv<R, V> r;                                                                                 \
+    _Pragma("unroll") for (int i = 0; i < V; i++) r.x[i] = a op b.x[i];                         \
+    return r;                                                                                   \
+  }                                                                                             \
+  template <typename R, int V>                                                                  \
+  __device__ __forceinline__ Mv<R, V> operator op(const Mv<R, V> &a, R b) {                     \
+    Mv<R, V> r;                                                                                 \
+    _Pragma("unroll") for (int i = 0; i < V; i++) r.x[i] = a.x[i] op b;                         \
+    return r;                                                                                   \
+  }
+MPSW_MV_OP(+)
+MPSW_MV_OP(-)
+MPSW_MV_OP(*)
+MPSW_MV_OP(/)
+#undef MPSW_MV_OP
+
+template <typename R, int V>
+__device__ __forceinline__ Mv<R, V> operator-(const Mv<R, V> &a) {
+  Mv<R, V> r;
+#pragma unroll
+  for (int i = 0; i < V; i++) r.x[i] = -a.x[i];
+  return r;
+}
+
+template <typename R, int V>
+__device__ __forceinline__ Mv<R, V> mv_fill(R a) {
+  Mv<R, V> r;
+#pragma unroll
+  for (int i = 0; i < V; i++) r.x[i] = a;
+  return r;
+}
+
+// vector load / store of V consecutive members (the offset is a multiple of V)
+template <int V, typename R>
+__device__ __forceinline__ Mv<R, V> ldv(const R *p) {
+  return *reinterpret_cast<const Mv<R, V> *>(p);
+}
+template <int V, typename R>
+__device__ __forceinline__ void stv(R *p, const Mv<R, V> &v) {
+  *reinterpret_cast<Mv<R, V> *>(p) = v;
+}
+
+template <int V, typename D, typename S>
+__device__ __forceinline__ Mv<D, V> mv_cast(const Mv<S, V> &a) {
+  Mv<D, V> r;
+#pragma unroll
+  for (int i = 0; i < V; i++) r.x[i] = D(a.x[i]);
+  return r;
+}
+
+// thread t -> (entity, first member)
+#define MPSW_MEMBER_LOOP(t, n, B, V)                                      \
+  MPSW_GRID_LOOP(t, (long long)(n) * ((B) / (V)))
+
+struct EntMember {
+  int ent, b;
+};
+__device__ __forceinline__ EntMember ent_member(long long t, int B, int V) {
+  const int bv = B / V;
+  const int ent = (int)(t / bv);
+  return {ent, (int)(t - (long long)ent * bv) * V};
+}
+
+// RK4 bookkeeping of V members (src/mpas_sw_module.f90:590-611)
+template <typename R, typename A, int V>
+__device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const Mv<R, V> &t) {
+  if (rk.next) {
+    const Mv<A, V> x0 = ldv<V>(rk.x0 + o);
+    Mv<R, V> n;
+#pragma unroll
+    for (int i = 0; i < V; i++) n.x[i] = rk.frozen ? R(x0.x[i]) : R(x0.x[i] + rk.c * A(t.x[i]));
+    stv<V>(rk.next + o, n);
+  }
+  if (rk.acc_out && !rk.frozen) {
+    Mv<A, V> a = ldv<V>(rk.acc_in + o);
+#pragma unroll
+    for (int i = 0; i < V; i++) a.x[i] = a.x[i] + rk.w * A(t.x[i]);
+    stv<V>(rk.acc_out + o, a);
+  }
+}
+
+// del4 intermediates (src/mpas_sw_dyncore.f90:554-589): delsq_vorticity on vertices and
+// delsq_divergence on cells.  One grid covers the vertex threads followed by the cell threads.
+template <typename R, int V>
+__global__ void k_del4_vc(MeshDev<R> m, int B, const R *__restrict__ dsq_u, R *dsq_vort, R *dsq_div) {
+  using M = Mv<R, V>;
+  const int nV = m.nV, nC = m.nC;
+  const long long tv = (long long)nV * (B / V);
+  MPSW_GRID_LOOP(t, tv + (long long)nC * (B / V)) {
+    if (t < tv) {
+      const EntMember q = ent_member(t, B, V);
+      const int v = q.ent;
+      M dcirc = mv_fill<R, V>(R(0));
+#pragma unroll
+      for (int k = 0; k < VDEG; k++) {
+        const int e = ld(m.v_es, (size_t)k * nV + v);
+        const R s = R(m.v_esg[(size_t)k * nV + v]);
+        dcirc = dcirc + s * (ld(m.e_dc, e) * ldv<V>(dsq_u + (size_t)e * B + q.b));
+      }
+      stv<V>(dsq_vort + (size_t)v * B + q.b, dcirc * (R(1) / ld(m.v_area, v)));
+    } else {
+      const EntMember q = ent_member(t - tv, B, V);
+      const int c = q.ent;
+      const int n = ld(m.c_n, c);
+      M dd = mv_fill<R, V>(R(0));
+      for (int k = 0; k < n; k++) {
+        const int e = ld(m.c_es, (size_t)k * nC + c);
+        const R s = R(m.c_esg[(size_t)k * nC + c]);
+        dd = dd + s * (ldv<V>(dsq_u + (size_t)e * B + q.b) * ld(m.e_dv, e));
+      }
+      stv<V>(dsq_div + (size_t)c * B + q.b, dd * (R(1) / ld(m.c_area, c)));
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Tangent linear (src/mpas_sw_dyncore_tlm.f90)
+// ----------------------------------------------------------------------------------------
+
+// :255-271 and :344-360
+template <typename R, int V>
+__global__ void k_tl_vertex(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                            const R *__restrict__ ht, Diag<R> d) {
+  using M = Mv<R, V>;
+  const int nV = m.nV;
+  MPSW_MEMBER_LOOP(t, nV, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int v = q.ent;
+    M circ = mv_fill<R, V>(R(0));
+#pragma unroll
+    for (int k = 0; k < VDEG; k++) {
+      const int e = ld(m.v_es, (size_t)k * nV + v);
+      const R s = R(m.v_esg[(size_t)k * nV + v]);
+      circ = circ + s * (ld(m.e_dc, e) * ldv<V>(ut + (size_t)e * B + q.b));
+    }
+    const R area = ld(m.v_area, v);
+    const M vort = circ / area;
+    M hvt = mv_fill<R, V>(R(0));
+#pragma unroll
+    for (int k = 0; k < VDEG; k++)
+      hvt = hvt + ldv<V>(ht + (size_t)ld(m.v_c, (size_t)k * nV + v) * B + q.b) * ld(m.v_k, (size_t)k * nV + v);
+    hvt = hvt / area;
+    const R hv = ld(bs.hv, v);
+    const M pvt = vort / hv - (hvt * (ld(m.v_f, v) + ld(bs.vort, v))) / (hv * hv);
+    const size_t o = (size_t)v * B + q.b;
+    if (d.circ) stv<V>(d.circ + o, circ);
+    stv<V>(d.vort + o, vort);
+    if (d.hv) stv<V>(d.hv + o, hvt);
+    stv<V>(d.pvv + o, pvt);
+  }
+}
+
+// :274-316, :397-421, thickness tendency :541-561 and the RK update
+template <typename R, typename A, int V>
+__global__ void k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                          const R *__restrict__ ht, Diag<R> d, RK<R, A> rk, R *tend_h) {
+  using M = Mv<R, V>;
+  const int nC = m.nC;
+  MPSW_MEMBER_LOOP(t, nC, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int c = q.ent;
+    const int n = ld(m.c_n, c);
+    M div = mv_fill<R, V>(R(0)), th = mv_fill<R, V>(R(0));
+    for (int k = 0; k < n; k++) {
+      const int e = ld(m.c_es, (size_t)k * nC + c);
+      const R s = R(m.c_esg[(size_t)k * nC + c]);
+      const M ue = ldv<V>(ut + (size_t)e * B + q.b);
+      const R dve = ld(m.e_dv, e);
+      div = div + s * (ue * dve);
+      const M het = R(0.5) * (ldv<V>(ht + (size_t)ld(m.e_c1, e) * B + q.b) +
+                              ldv<V>(ht + (size_t)ld(m.e_c2, e) * B + q.b));
+      const M flux = (ue * dve) * ld(bs.he, e) + (ld(bs.u, e) * dve) * het;
+      th = th + (-s) * flux;
+    }
+    const R area = ld(m.c_area, c);
+    div = div * (R(1) / area);
+    M ke = mv_fill<R, V>(R(0));
+    for (int i = 0; i < n; i++) {
+      const int e = ld(m.c_eoc, (size_t)i * nC + c);
+      ke = ke + ((R(0.25) * ld(m.e_dc, e)) * ld(m.e_dv, e)) * ((R(2) * ld(bs.u, e)) * ldv<V>(ut + (size_t)e * B + q.b));
+    }
+    ke = ke / area;
+    M pc = mv_fill<R, V>(R(0)), vc = mv_fill<R, V>(R(0));
+    for (int k = 0; k < n; k++) {
+      const int v = ld(m.c_vs, (size_t)k * nC + c);
+      const R kt = ld(m.c_vk, (size_t)k * nC + c);
+      pc = pc + (kt * ldv<V>(d.pvv + (size_t)v * B + q.b)) / area;
+      if (d.vc) vc = vc + (kt * ldv<V>(d.vort + (size_t)v * B + q.b)) / area;
+    }
+    th = th / area;
+    const size_t o = (size_t)c * B + q.b;
+    stv<V>(d.div + o, div);
+    stv<V>(d.ke + o, ke);
+    stv<V>(d.pc + o, pc);
+    if (d.vc) stv<V>(d.vc + o, vc);
+    if (tend_h) stv<V>(tend_h + o, th);
+    rk_members<R, A, V>(rk, o, th);
+  }
+}
+
+// :319-329, :364-393, :425-445, h_edge_tl :117-126, delsq_u_tl :638-652
+template <typename R, int V>
+__global__ void k_tl_edge_diag(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                               const R *__restrict__ ht, Diag<R> d, Phys<R> ph) {
+  using M = Mv<R, V>;
+  const int nE = m.nE;
+  MPSW_MEMBER_LOOP(t, nE, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int e = q.ent;
+    const int n = ld(m.e_n, e);
+    M vt = mv_fill<R, V>(R(0));
+    for (int j = 0; j < n; j++)
+      vt = vt + ld(m.e_w, (size_t)j * nE + e) * ldv<V>(ut + (size_t)ld(m.e_eoe, (size_t)j * nE + e) * B + q.b);
+    const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
+    const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
+    const M gptt = (ldv<V>(d.pvv + (size_t)v2 * B + q.b) - ldv<V>(d.pvv + (size_t)v1 * B + q.b)) / dv;
+    M pet = mv_fill<R, V>(R(0));
+    pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_va, e) * B + q.b);
+    pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_vb, e) * B + q.b);
+    pet = pet - ((ph.apvm * vt) * ph.dt) * ld(bs.gpt, e) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * gptt;
+    const M gpnt = (ldv<V>(d.pc + (size_t)c2 * B + q.b) - ldv<V>(d.pc + (size_t)c1 * B + q.b)) / dc;
+    const M uet = ldv<V>(ut + (size_t)e * B + q.b);
+    pet = pet - ((ph.apvm * uet) * ph.dt) * ld(bs.gpn, e) - ((ph.apvm * ld(bs.u, e)) * ph.dt) * gpnt;
+    const size_t o = (size_t)e * B + q.b;
+    stv<V>(d.pe + o, pet);
+    stv<V>(d.he + o, R(0.5) * (ldv<V>(ht + (size_t)c1 * B + q.b) + ldv<V>(ht + (size_t)c2 * B + q.b)));
+    if (d.v) stv<V>(d.v + o, vt);
+    if (d.gpt) stv<V>(d.gpt + o, gptt);
+    if (d.gpn) stv<V>(d.gpn + o, gpnt);
+    if (d.dsq_u)
+      stv<V>(d.dsq_u + o, (ldv<V>(d.div + (size_t)c2 * B + q.b) - ldv<V>(d.div + (size_t)c1 * B + q.b)) / dc -
+                              (ldv<V>(d.vort + (size_t)v2 * B + q.b) - ldv<V>(d.vort + (size_t)v1 * B + q.b)) / dv);
+  }
+}
+
+// sw_compute_tend_tlm normal-velocity part :564-768 and the RK update
+template <typename R, typename A, int V>
+__global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                               const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
+                               R *tend_u) {
+  using M = Mv<R, V>;
+  const int nE = m.nE;
+  MPSW_MEMBER_LOOP(t, nE, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int e = q.ent;
+    const int n = ld(m.e_n, e);
+    const M pet_e = ldv<V>(d.pe + (size_t)e * B + q.b);
+    const R pe_e = ld(bs.pe, e);
+    M qt = mv_fill<R, V>(R(0));
+    for (int j = 0; j < n; j++) {
+      const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
+      const R w = ld(m.e_w, (size_t)j * nE + e);
+      const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + q.b));
+      const R wpv = R(0.5) * (pe_e + ld(bs.pe, eoe));
+      const R ub = ld(bs.u, eoe), heb = ld(bs.he, eoe);
+      qt = qt + ((w * ldv<V>(ut + (size_t)eoe * B + q.b)) * wpv) * heb + ((w * ub) * wpvt) * heb +
+           ((w * ub) * wpv) * ldv<V>(d.he + (size_t)eoe * B + q.b);
+    }
+    const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
+    const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
+    M tut = qt - ((ldv<V>(d.ke + (size_t)c2 * B + q.b) - ldv<V>(d.ke + (size_t)c1 * B + q.b)) +
+                  R(GRAVITY) * (ldv<V>(ht + (size_t)c2 * B + q.b) - ldv<V>(ht + (size_t)c1 * B + q.b))) / dc;
+    if (ph.visc2 > R(0)) {
+      M ud = (ldv<V>(d.div + (size_t)c2 * B + q.b) - ldv<V>(d.div + (size_t)c1 * B + q.b)) / dc -
+             (ldv<V>(d.vort + (size_t)v2 * B + q.b) - ldv<V>(d.vort + (size_t)v1 * B + q.b)) / dv;
+      ud = (ld(m.e_sc2, e) * ph.visc2) * ud;
+      tut = tut + ud;
+    }
+    if (ph.visc4 > R(0)) {
+      M ud = (ldv<V>(d.dsq_div + (size_t)c2 * B + q.b) - ldv<V>(d.dsq_div + (size_t)c1 * B + q.b)) / dc -
+             (ldv<V>(d.dsq_vort + (size_t)v2 * B + q.b) - ldv<V>(d.dsq_vort + (size_t)v1 * B + q.b)) / dv;
+      ud = (ld(m.e_sc4, e) * ph.visc4) * ud;
+      tut = tut - ud;
+    }
+    const R hh = ld(bs.he, e);
+    const M het = ldv<V>(d.he + (size_t)e * B + q.b);
+    if (ph.wind) tut = tut - ((het * ld(m.e_usrc, e)) / R(RHO_REF)) / (hh * hh);
+    if (ph.drag) {
+      const M ket_e = R(0.5) * (ldv<V>(d.ke + (size_t)c1 * B + q.b) + ldv<V>(d.ke + (size_t)c2 * B + q.b));
+      const R ke_e = R(0.5) * (ld(bs.ke, c1) + ld(bs.ke, c2));
+      const R uu = ld(bs.u, e), sq = sqrt(R(2) * ke_e);
+      tut = tut - ((R(1.0e-3) * ldv<V>(ut + (size_t)e * B + q.b)) * sq) / hh -
+            ((((R(0.5) * R(1.0e-3)) * uu) * (R(2) * ket_e)) / sq) / hh +
+            (((R(1.0e-3) * uu) * sq) * het) / (hh * hh);
+    }
+    const size_t o = (size_t)e * B + q.b;
+    if (tend_u) stv<V>(tend_u + o, tut);
+    rk_members<R, A, V>(rk, o, tut);
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Adjoint of one RK stage (src/mpas_sw_dyncore_adj.f90): sw_compute_tend_adj (:455-738)
+// followed by sw_compute_solve_diagnostics_adj (:1-453) at the same linearisation point,
+// as gathers over transposed connectivity; no atomics.
+// ----------------------------------------------------------------------------------------
+
+// Tendency adjoint of the last stage of a step (src/mpas_sw_module.f90:912-914 at rk=4):
+// tu = wu * x2u + seed_tu, th = (wh * x2h + seed_th) / areaCell.  Edge threads then cell threads.
+template <typename R, typename A, int V>
+__global__ void k_ad_tinit(MeshDev<R> m, int B, const A *x2u, const A *x2h, const R *seed_tu,
+                           const R *seed_th, A wu, A wh, R *tu, R *th) {
+  const long long te = (long long)m.nE * (B / V);
+  MPSW_GRID_LOOP(t, te + (long long)m.nC * (B / V)) {
+    if (t < te) {
+      const EntMember q = ent_member(t, B, V);
+      const size_t o = (size_t)q.ent * B + q.b;
+      Mv<R, V> r;
+#pragma unroll
+      for (int i = 0; i < V; i++) {
+        A x = x2u ? wu * x2u[o + i] : A(0);
+        if (seed_tu) x = x + A(seed_tu[q.ent]);
+        r.x[i] = R(x);
+      }
+      stv<V>(tu + o, r);
+    } else {
+      const EntMember q = ent_member(t - te, B, V);
+      const size_t o = (size_t)q.ent * B + q.b;
+      const A area = A(ld(m.c_area, q.ent));
+      Mv<R, V> r;
+#pragma unroll
+      for (int i = 0; i < V; i++) {
+        A x = x2h ? wh * x2h[o + i] : A(0);
+        if (seed_th) x = x + A(seed_th[q.ent]);
+        r.x[i] = R(x / area);
+      }
+      stv<V>(th + o, r);
+    }
+  }
+}
+
+// Edge stage: workpv/q adjoint (:689-718) as a gather over the transposed edgesOnEdge,
+// thickness-flux adjoint (:720-736), drag (:549-565), wind (:567-572), then the APVM adjoints
+// of the diagnostics (:193-200, :235-242).
+template <typename R, typename A, int V>
+__global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+                          AdWork<R> w) {
+  using M = Mv<R, V>;
+  const int nE = m.nE;
+  MPSW_MEMBER_LOOP(t, nE, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int e = q.ent;
+    const int n = ld(m.e_n, e);
+    const M Te = ldv<V>(in.tu + (size_t)e * B + q.b);
+    const R ue = ld(bs.u, e), hee = ld(bs.he, e), pee = ld(bs.pe, e);
+    M pe_ad = mv_fill<R, V>(R(0)), he_ad = mv_fill<R, V>(R(0)), ud = mv_fill<R, V>(R(0));
+    for (int j = 0; j < n; j++) {
+      const int nb = ld(m.e_eoe, (size_t)j * nE + e);
+      const R wj = ld(m.e_w, (size_t)j * nE + e);
+      const R wr = ld(m.e_wrev, (size_t)j * nE + e);
+      pe_ad = pe_ad + R(0.5) * (((wj * ld(bs.u, nb)) * ld(bs.he, nb)) * Te);
+      const M Tn = ldv<V>(in.tu + (size_t)nb * B + q.b);
+      const R wpv = R(0.5) * (ld(bs.pe, nb) + pee);
+      he_ad = he_ad + ((wr * ue) * wpv) * Tn;
+      pe_ad = pe_ad + R(0.5) * (((wr * ue) * hee) * Tn);
+      ud = ud + ((wr * wpv) * hee) * Tn;
+    }
+    const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
+    const R dv = ld(m.e_dv, e);
+    const M fa = ldv<V>(in.th + (size_t)c2 * B + q.b) - ldv<V>(in.th + (size_t)c1 * B + q.b);
+    he_ad = he_ad + (ue * dv) * fa;
+    ud = ud + (dv * hee) * fa;
+    if (ph.drag) {
+      const R sq = sqrt(R(2) * (R(0.5) * (ld(bs.ke, c1) + ld(bs.ke, c2))));
+      he_ad = he_ad + (((R(1.0e-3) * ue) * sq) / (hee * hee)) * Te;
+      ud = ud - ((R(1.0e-3) * sq) / hee) * Te;
+    }
+    if (ph.wind) he_ad = he_ad - ((ld(m.e_usrc, e) / R(RHO_REF)) / (hee * hee)) * Te;
+    M gpn_ad = mv_fill<R, V>(R(0)), gpt_ad = mv_fill<R, V>(R(0)), v_ad = mv_fill<R, V>(R(0));
+    if (sd.pe) pe_ad = pe_ad + sd.pe[e];
+    if (sd.he) he_ad = he_ad + sd.he[e];
+    if (sd.gpn) gpn_ad = mv_fill<R, V>(sd.gpn[e]);
+    if (sd.gpt) gpt_ad = mv_fill<R, V>(sd.gpt[e]);
+    if (sd.v) v_ad = mv_fill<R, V>(sd.v[e]);
+    gpn_ad = gpn_ad - ((ph.apvm * ue) * ph.dt) * pe_ad;
+    ud = ud - ((ph.apvm * ph.dt) * ld(bs.gpn, e)) * pe_ad;
+    gpt_ad = gpt_ad - ((ph.apvm * ld(bs.v, e)) * ph.dt) * pe_ad;
+    v_ad = v_ad - ((ph.apvm * ph.dt) * ld(bs.gpt, e)) * pe_ad;
+    const size_t o = (size_t)e * B + q.b;
+    stv<V>(w.pe_ad + o, pe_ad);
+    stv<V>(w.he_ad + o, he_ad);
+    stv<V>(w.ud + o, ud);
+    stv<V>(w.gpn_ad + o, gpn_ad);
+    stv<V>(w.gpt_ad + o, gpt_ad);
+    stv<V>(w.v_ad + o, v_ad);
+  }
+}
+
+// del4 adjoint, first half (:588-634): delsq_vorticity/delsq_circulation adjoint on vertices
+// and delsq_divergence adjoint on cells.
+template <typename R, int V>
+__global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R> in, AdWork<R> w) {
+  using M = Mv<R, V>;
+  const int nV = m.nV, nC = m.nC;
+  const long long tv = (long long)nV * (B / V);
+  MPSW_GRID_LOOP(t, tv + (long long)nC * (B / V)) {
+    if (t < tv) {
+      const EntMember q = ent_member(t, B, V);
+      const int v = q.ent;
+      M acc = mv_fill<R, V>(R(0));
+#pragma unroll
+      for (int k = 0; k < VDEG; k++) {
+        const int e = ld(m.v_es, (size_t)k * nV + v);
+        const R sg = R(m.v_esg[(size_t)k * nV + v]);
+        const M ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-ldv<V>(in.tu + (size_t)e * B + q.b));
+        acc = acc + (-sg) * (ud4 / ld(m.e_dv, e));
+      }
+      stv<V>(w.dc_ad + (size_t)v * B + q.b, acc * (R(1) / ld(m.v_area, v)));
+    } else {
+      const EntMember q = ent_member(t - tv, B, V);
+      const int c = q.ent;
+      const int n = ld(m.c_n, c);
+      M acc = mv_fill<R, V>(R(0));
+      for (int k = 0; k < n; k++) {
+        const int e = ld(m.c_es, (size_t)k * nC + c);
+        const R sg = R(m.c_esg[(size_t)k * nC + c]);
+        const M ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-ldv<V>(in.tu + (size_t)e * B + q.b));
+        acc = acc + (-sg) * (ud4 / ld(m.e_dc, e));
+      }
+      stv<V>(w.dd_ad + (size_t)c * B + q.b, acc * (R(1) / ld(m.c_area, c)));
+    }
+  }
+}
+
+// del4 adjoint, second half (:617-643): delsq_u adjoint on edges.
+template <typename R, int V>
+__global__ void k_ad_del4_e(MeshDev<R> m, int B, AdWork<R> w) {
+  using M = Mv<R, V>;
+  const int nE = m.nE;
+  MPSW_MEMBER_LOOP(t, nE, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int e = q.ent;
+    const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
+    M du = mv_fill<R, V>(R(0));
+    du = du - dv * ldv<V>(w.dd_ad + (size_t)ld(m.e_c2, e) * B + q.b);
+    du = du + dv * ldv<V>(w.dd_ad + (size_t)ld(m.e_c1, e) * B + q.b);
+    du = du + dc * ldv<V>(w.dc_ad + (size_t)ld(m.e_v2, e) * B + q.b);
+    du = du - dc * ldv<V>(w.dc_ad + (size_t)ld(m.e_v1, e) * B + q.b);
+    stv<V>(w.du_ad + (size_t)e * B + q.b, du);
+  }
+}
+
+// Cell stage: gradPVn adjoint onto pv_cell (:202-213), gravity/ke terms of the tendency
+// adjoint (:696-699), drag ke terms, del2/del4 divergence adjoints, h_edge adjoint (:358-369),
+// then the 1/areaCell scalings of ke_ad and divergence_ad (:306-326).
+template <typename R, typename A, int V>
+__global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+                          AdWork<R> w) {
+  using M = Mv<R, V>;
+  const int nC = m.nC;
+  MPSW_MEMBER_LOOP(t, nC, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int c = q.ent;
+    const int n = ld(m.c_n, c);
+    M pc_ad = mv_fill<R, V>(sd.pc ? sd.pc[c] : R(0));
+    M ke_ad = mv_fill<R, V>(sd.ke ? sd.ke[c] : R(0));
+    M div_ad = mv_fill<R, V>(sd.div ? sd.div[c] : R(0));
+    M hd = mv_fill<R, V>(R(0));
+    for (int k = 0; k < n; k++) {
+      const int e = ld(m.c_es, (size_t)k * nC + c);
+      const R sg = R(m.c_esg[(size_t)k * nC + c]);
+      const size_t oe = (size_t)e * B + q.b;
+      const M Te = ldv<V>(in.tu + oe);
+      const R dce = ld(m.e_dc, e);
+      pc_ad = pc_ad + (-sg) * (ldv<V>(w.gpn_ad + oe) / dce);
+      ke_ad = ke_ad + sg * (Te / dce);
+      hd = hd + sg * ((R(GRAVITY) / dce) * Te);
+      if (ph.drag) {
+        const R sq = sqrt(R(2) * (R(0.5) * (ld(bs.ke, ld(m.e_c1, e)) + ld(bs.ke, ld(m.e_c2, e)))));
+        const M kea = -(((((R(0.5) * R(1.0e-3)) * ld(bs.u, e)) * R(2)) / sq) / ld(bs.he, e)) * Te;
+        ke_ad = ke_ad + R(0.5) * kea;
+      }
+      if (ph.visc2 > R(0)) {
+        const M ud2 = (ld(m.e_sc2, e) * ph.visc2) * Te;
+        div_ad = div_ad + (-sg) * (ud2 / dce);
+      }
+      if (ph.visc4 > R(0)) div_ad = div_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dce);
+      hd = hd + R(0.5) * ldv<V>(w.he_ad + oe);
+    }
+    const R area = ld(m.c_area, c);
+    const size_t o = (size_t)c * B + q.b;
+    stv<V>(w.pc_ad + o, pc_ad);
+    stv<V>(w.ke_ad + o, ke_ad / area);
+    stv<V>(w.div_ad + o, div_ad * (R(1) / area));
+    stv<V>(w.hd + o, hd);
+  }
+}
+
+// Vertex stage: pv_cell -> pv_vertex (:215-229), pv_edge -> pv_vertex (:244-252),
+// gradPVt -> pv_vertex (:254-262), del2/del4 vorticity adjoints, pv_vertex -> h_vertex and
+// vorticity (:268-284), vorticity -> circulation (:343-349).
+template <typename R, typename A, int V>
+__global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in,
+                            AdSeeds<R> sd, AdWork<R> w) {
+  using M = Mv<R, V>;
+  const int nV = m.nV;
+  MPSW_MEMBER_LOOP(t, nV, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    const int v = q.ent;
+    M pvv_ad = mv_fill<R, V>(sd.pvv ? sd.pvv[v] : R(0));
+    M vort_ad = mv_fill<R, V>(sd.vort ? sd.vort[v] : R(0));
+#pragma unroll
+    for (int i = 0; i < VDEG; i++) {
+      const int c = ld(m.v_c, (size_t)i * nV + v);
+      const R ka = ld(m.v_k, (size_t)i * nV + v) / ld(m.c_area, c);
+      if (sd.vc) vort_ad = vort_ad + ka * sd.vc[c];
+      pvv_ad = pvv_ad + ka * ldv<V>(w.pc_ad + (size_t)c * B + q.b);
+    }
+#pragma unroll
+    for (int i = 0; i < VDEG; i++)
+      pvv_ad = pvv_ad + R(0.5) * ldv<V>(w.pe_ad + (size_t)ld(m.v_e, (size_t)i * nV + v) * B + q.b);
+#pragma unroll
+    for (int k = 0; k < VDEG; k++) {
+      const int e = ld(m.v_es, (size_t)k * nV + v);
+      const R sg = R(m.v_esg[(size_t)k * nV + v]);
+      const R dve = ld(m.e_dv, e);
+      const size_t oe = (size_t)e * B + q.b;
+      pvv_ad = pvv_ad + sg * (ldv<V>(w.gpt_ad + oe) / dve);
+      if (ph.visc2 > R(0)) {
+        const M ud2 = (ld(m.e_sc2, e) * ph.visc2) * ldv<V>(in.tu + oe);
+        vort_ad = vort_ad + (-sg) * (ud2 / dve);
+      }
+      if (ph.visc4 > R(0)) vort_ad = vort_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dve);
+    }
+    const R hv = ld(bs.hv, v), area = ld(m.v_area, v);
+    M hv_ad = mv_fill<R, V>(sd.hv ? sd.hv[v] : R(0));
+    hv_ad = hv_ad - ((ld(m.v_f, v) + ld(bs.vort, v)) / (hv * hv)) * pvv_ad;
+    vort_ad = vort_ad + pvv_ad / hv;
+    hv_ad = hv_ad / area;
+    const M circ_ad = mv_fill<R, V>(sd.circ ? sd.circ[v] : R(0)) + vort_ad / area;
+    const size_t o = (size_t)v * B + q.b;
+    stv<V>(w.hv_ad + o, hv_ad);
+    stv<V>(w.circ_ad + o, circ_ad);
+  }
+}
+
+template <typename R, typename A, int V>
+__device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, size_t o, const Mv<R, V> &pad,
+                                        R area) {
+  A *acc = is_edge ? out.acc_u : out.acc_h;
+  const A *x2 = is_edge ? out.x2u : out.x2h;
+  R *tn = is_edge ? out.tu_next : out.th_next;
+  const A wn = is_edge ? out.wu : out.wh, cn = is_edge ? out.cu : out.ch;
+  Mv<A, V> next;
+  if (out.mode == AD_FINAL) {
+    A *dst = is_edge ? out.dst_u : out.dst_h;
+    const Mv<A, V> a = ldv<V>(acc + o), x = ldv<V>(x2 + o);
+    Mv<A, V> d;
+#pragma unroll
+    for (int i = 0; i < V; i++) {
+      d.x[i] = (a.x[i] + x.x[i]) + A(pad.x[i]);
+      next.x[i] = wn * d.x[i];
+    }
+    stv<V>(dst + o, d);
+  } else {
+    Mv<A, V> a;
+    if (out.mode == AD_SET) {
+      a = mv_cast<V, A>(pad);
+    } else {
+      a = ldv<V>(acc + o);
+#pragma unroll
+      for (int i = 0; i < V; i++) a.x[i] = a.x[i] + A(pad.x[i]);
+    }
+    stv<V>(acc + o, a);
+    if (tn) {
+      const Mv<A, V> x = x2 ? ldv<V>(x2 + o) : mv_fill<A, V>(A(0));
+#pragma unroll
+      for (int i = 0; i < V; i++) next.x[i] = (x2 ? wn * x.x[i] : A(0)) + cn * A(pad.x[i]);
+    }
+  }
+  if (tn) {
+    Mv<R, V> r;
+#pragma unroll
+    for (int i = 0; i < V; i++) r.x[i] = is_edge ? R(next.x[i]) : R(next.x[i] / A(area));
+    stv<V>(tn + o, r);
+  }
+}
+
+// Final stage of the adjoint: h_vertex -> h (:286-289) on cells, and on edges the transposed
+// tangential velocity (:296-303), ke (:306-317), divergence (:327-340) and circulation
+// (:350-355) adjoints.  Cell threads then edge threads.
+template <typename R, typename A, int V>
+__global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out) {
+  using M = Mv<R, V>;
+  const int nC = m.nC, nE = m.nE;
+  const long long tc = (long long)nC * (B / V);
+  MPSW_GRID_LOOP(t, tc + (long long)nE * (B / V)) {
+    if (t < tc) {
+      const EntMember q = ent_member(t, B, V);
+      const int c = q.ent;
+      const int n = ld(m.c_n, c);
+      M ph_ = ldv<V>(w.hd + (size_t)c * B + q.b);
+      for (int k = 0; k < n; k++)
+        ph_ = ph_ + ld(m.c_vk, (size_t)k * nC + c) * ldv<V>(w.hv_ad + (size_t)ld(m.c_vs, (size_t)k * nC + c) * B + q.b);
+      ad_emit<R, A, V>(out, 0, (size_t)c * B + q.b, ph_, ld(m.c_area, c));
+    } else {
+      const EntMember q = ent_member(t - tc, B, V);
+      const int e = q.ent;
+      const int n = ld(m.e_n, e);
+      M pu = ldv<V>(w.ud + (size_t)e * B + q.b);
+      for (int j = 0; j < n; j++) {
+        const int nb = ld(m.e_eoe, (size_t)j * nE + e);
+        pu = pu + ld(m.e_wrev, (size_t)j * nE + e) * ldv<V>(w.v_ad + (size_t)nb * B + q.b);
+      }
+      const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
+      const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
+      const R kc = (((R(0.25) * dc) * dv) * R(2)) * ld(bs.u, e);
+      pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c1 * B + q.b);
+      pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c2 * B + q.b);
+      pu = pu - dv * ldv<V>(w.div_ad + (size_t)c2 * B + q.b);
+      pu = pu + dv * ldv<V>(w.div_ad + (size_t)c1 * B + q.b);
+      pu = pu + dc * ldv<V>(w.circ_ad + (size_t)v2 * B + q.b);
+      pu = pu - dc * ldv<V>(w.circ_ad + (size_t)v1 * B + q.b);
+      ad_emit<R, A, V>(out, 1, (size_t)e * B + q.b, pu, R(1));
+    }
+  }
+}
+
+}  // namespace mpsw
