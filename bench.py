@@ -42,6 +42,8 @@ def parse():
     p.add_argument('--nsteps', type=int, default=288)
     p.add_argument('--dt', type=float, default=300.0)
     p.add_argument('--ckpt', type=int, default=16)
+    p.add_argument('--storage', type=int, default=-1,
+                   help='stage storage mode of the window: -1 auto, 0 checkpoints only, 1 FP64, 2 FP32, 3 both')
     p.add_argument('--no-plain', action='store_true', help='skip the plain FP64 arm')
     p.add_argument('--profile', action='store_true',
                    help='only the timed batched windows (for profiler launch lists); no JSON line')
@@ -260,7 +262,7 @@ def run_mpsw(a, rank, world):
 
     def gradient_batch(prec, Bm, u0, h0):
         """One bench step on device-resident members: window, TL, AD seeded with the TL output."""
-        w = Window(eng, a.nsteps, a.ckpt)
+        w = Window(eng, a.nsteps, a.ckpt, a.storage)
         xu, xh = u0.clone(), h0.clone()
         w.tl_internal(xu, xh, prec)
         w.ad_internal(xu, xh, prec)
@@ -322,7 +324,7 @@ def run_mpsw(a, rank, world):
     out_h = torch.empty_like(dh_host).pin_memory()
 
     def e2e_step():
-        w = Window(eng, a.nsteps, a.ckpt)
+        w = Window(eng, a.nsteps, a.ckpt, a.storage)
         xu = du_host.to('cuda', non_blocking=True)
         xh = dh_host.to('cuda', non_blocking=True)
         tu, th = w.tl(xu, xh, FP32)
@@ -375,6 +377,7 @@ def run_mpsw(a, rank, world):
             'vs_baseline': None, 'dtype': 'f32 stencils + f64 accumulation',
             'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh, seeded perturbations)' % a.level,
             'config': {'workload': 'TL+AD window: level-%d mesh (%d cells), %d RK4 steps of %g s, %d members, checkpoint every %d' % (a.level, nC, a.nsteps, a.dt, B, a.ckpt),
+                       'stage_storage': {-1: 'auto (FP64+FP32 stage linearisation points when they fit 40%% of free HBM)', 0: 'none: stages recomputed from checkpoints', 1: 'FP64', 2: 'FP32', 3: 'FP64+FP32'}[a.storage],
                        'members_per_gpu': B, 'parallelism': 'replicas x%d' % world,
                        'l2': 'flushed (256 MB write) between timed steps; working set ~%.0f MB' % wset},
             'fp64_plain_gradients_per_s': plain,

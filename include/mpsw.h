@@ -94,10 +94,19 @@ int mpsw_state_from_device(mpsw_handle *h, const double *u, const double *hh, vo
 int mpsw_state_to_device(mpsw_handle *h, double *u, double *hh, void *stream);
 
 /* A window of `nsteps` RK4 steps starting from the current level-1 state u(1), h(1) (which is
- * left unchanged).  The nonlinear trajectory is stored as checkpoints every `ckpt_every`
- * steps; tangent-linear and adjoint sweeps recompute states and RK stages from them.
+ * left unchanged).  The nonlinear trajectory is kept as checkpoints every `ckpt_every` steps
+ * and, as the storage mode selects, as the linearisation point of every RK stage of every
+ * step; tangent-linear and adjoint sweeps read stored stages, or recompute states and stages
+ * from the checkpoints where that precision is not stored (identical results either way).
  * precision: 0 = FP64 throughout, 1 = FP32 stencils with FP64 RK accumulation. */
 int mpsw_window_init(mpsw_handle *h, int nsteps, int ckpt_every, void *stream);
+/* Storage mode of the following mpsw_window_init calls.  No counterpart in the reference
+ * (sw_rk4_adj recomputes a step's stages from its start state).  mode -1 (default): store the
+ * FP64 and FP32 stage linearisation points when both fit in max_bytes (max_bytes 0: 40% of
+ * the free device memory), else the FP32 ones alone if they fit, else none; mode 0: none
+ * (checkpoints only); mode 1, 2, 3: FP64, FP32, both, regardless of size.  A stage slot holds
+ * 6 nEdges + 2 nVertices + nCells values, nsteps * 4 slots per stored precision. */
+int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes);
 /* Tangent linear over the window, B members in place: du [nEdges][B], dh [nCells][B]. */
 int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh, void *stream);
 /* Adjoint over the window, B members in place: on entry the adjoint of the final state, on

@@ -48,6 +48,18 @@ struct Window {
   double *su[4] = {}, *sh[4] = {};
   Diag<float> sd32[4];
   float *su32[4] = {};
+  // Stored linearisation points: the nine base fields of every RK stage of every step, per
+  // precision (0 FP64, 1 FP32).  A slot is one stage: u, h_edge, v, gradPVt, gradPVn, pv_edge
+  // (edges), vorticity, h_vertex (vertices), ke (cells), each padded to 64 elements.
+  struct Store {
+    void *mem = nullptr;
+    int cap = 0;       // steps the allocation holds
+    int valid = 0;     // steps written by the last forward pass (0: sweeps recompute)
+    size_t slot = 0;   // elements per stage slot
+    size_t off[9] = {};
+  } st[2];
+  int store_mode = -1;        // -1 automatic, else a mask of the precisions to store
+  double store_budget = 0;    // bytes for automatic mode (0: 40% of free device memory)
   // member buffers per precision (0 FP64, 1 FP32), allocated for the largest B seen
   struct Members {
     int B = 0;
@@ -61,11 +73,14 @@ struct Window {
 struct GraphKey {
   int kind = 0, prec = 0, B = 0;
   const void *p1 = nullptr, *p2 = nullptr;
+  const void *p3 = nullptr;
+  long long n2 = 0;
   double dt = 0, apvm = 0, visc2 = 0, visc4 = 0;
   int flags = 0;
   bool operator==(const GraphKey &o) const {
-    return kind == o.kind && prec == o.prec && B == o.B && p1 == o.p1 && p2 == o.p2 && dt == o.dt &&
-           apvm == o.apvm && visc2 == o.visc2 && visc4 == o.visc4 && flags == o.flags;
+    return kind == o.kind && prec == o.prec && B == o.B && p1 == o.p1 && p2 == o.p2 && p3 == o.p3 &&
+           n2 == o.n2 && dt == o.dt && apvm == o.apvm && visc2 == o.visc2 && visc4 == o.visc4 &&
+           flags == o.flags;
   }
 };
 struct GraphEntry {
@@ -170,6 +185,9 @@ struct Engine {
   void window_free();
   void window_free_trajectory();
   void window_init(int nsteps, int every, cudaStream_t s);
+  void window_storage(int mode, double max_bytes);
+  void window_store_alloc(int nsteps);
+  void window_store_free(int prec);
   void window_trajectory(cudaStream_t s);
   void window_tl(int prec, int B, double *du, double *dh, cudaStream_t s);
   void window_ad(int prec, int B, double *au, double *ah, cudaStream_t s);

@@ -148,9 +148,12 @@ struct AdOut {
 
 // Up to kConvMax double arrays rounded to float by one launch (see convert_list).
 constexpr int kConvMax = 10;
+// up to kConvMax FP64 arrays, each rounded to FP32 into dst[i] and/or copied into dst64[i]
+// (either may be null)
 struct ConvList {
   const double *src[kConvMax];
   float *dst[kConvMax];
+  double *dst64[kConvMax];
   long long n[kConvMax];
   int count;
 };

@@ -302,7 +302,12 @@ static __global__ void k_convert_list(ConvList L) {
   for (int i = 0; i < L.count; i++) {
     const double *__restrict__ s = L.src[i];
     float *__restrict__ d = L.dst[i];
-    MPSW_GRID_LOOP(t, L.n[i]) d[t] = float(s[t]);
+    double *__restrict__ d64 = L.dst64[i];
+    MPSW_GRID_LOOP(t, L.n[i]) {
+      const double x = s[t];
+      if (d) d[t] = float(x);
+      if (d64) d64[t] = x;
+    }
   }
 }
 

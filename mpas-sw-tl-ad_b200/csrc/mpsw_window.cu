@@ -112,6 +112,21 @@ Base<double> base_for<double>(const Window &W, int k) { return base64(W, k); }
 template <>
 Base<float> base_for<float>(const Window &W, int k) { return base32(W, k); }
 
+// Base fields of stage k of step n in the store of precision prec (R is its element type)
+template <typename R>
+R *store_field(const Window::Store &S, int n, int k, int f) {
+  return (R *)S.mem + ((size_t)n * 4 + k) * S.slot + S.off[f];
+}
+template <typename R>
+Base<R> stored_base(const Window &W, int prec, int n, int k) {
+  const Window::Store &S = W.st[prec];
+  Base<R> b{};
+  b.u = store_field<R>(S, n, k, 0); b.he = store_field<R>(S, n, k, 1); b.v = store_field<R>(S, n, k, 2);
+  b.gpt = store_field<R>(S, n, k, 3); b.gpn = store_field<R>(S, n, k, 4); b.pe = store_field<R>(S, n, k, 5);
+  b.vort = store_field<R>(S, n, k, 6); b.hv = store_field<R>(S, n, k, 7); b.ke = store_field<R>(S, n, k, 8);
+  return b;
+}
+
 template <typename R>
 const MeshDev<R> &mesh_for(const Engine &E);
 template <>
@@ -194,9 +209,74 @@ void Engine::window_free() {
   window_free_trajectory();
 }
 
+void Engine::window_store_free(int prec) {
+  Window::Store &S = win.st[prec];
+  if (S.mem) {
+    graphs_free();
+    cudaFree(S.mem);
+  }
+  S.mem = nullptr;
+  S.cap = S.valid = 0;
+}
+
+// Storage mode of the next windows: -1 automatic, 0 checkpoints only, or a mask of the
+// precisions whose linearisation points are stored (1 FP64, 2 FP32).
+void Engine::window_storage(int mode, double max_bytes) {
+  if (mode < -1 || mode > 3) throw EngineError(MPSW_ERR_ARG, "storage mode must be -1..3");
+  if (max_bytes < 0) throw EngineError(MPSW_ERR_ARG, "storage budget must be >= 0");
+  win.store_mode = mode;
+  win.store_budget = max_bytes;
+  for (int p = 0; p < 2; p++) win.st[p].valid = 0;  // takes effect at the next window_init
+}
+
+// (Re)allocate the stores of the precisions the storage mode selects for `nsteps` steps.  In
+// automatic mode FP64 and FP32 are both stored when they fit the budget, else FP32 alone when
+// it fits, else neither (the sweeps then recompute stages from checkpoints).
+void Engine::window_store_alloc(int nsteps) {
+  Window &W = win;
+  const size_t pad = 64;
+  auto up = [&](size_t n) { return (n + pad - 1) / pad * pad; };
+  size_t off[9], slot = 0;
+  for (int f = 0; f < 9; f++) {
+    off[f] = slot;
+    slot += up(f < 6 ? (size_t)nE : f < 8 ? (size_t)nV : (size_t)nC);
+  }
+  const size_t per = (size_t)nsteps * 4 * slot;
+  int mask = W.store_mode;
+  if (mask < 0) {
+    double budget = W.store_budget;
+    if (budget <= 0) {
+      size_t fr = 0, tot = 0;
+      cuda_check(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+      double held = 0;
+      for (int p = 0; p < 2; p++)
+        if (W.st[p].mem) held += (double)W.st[p].cap * 4 * W.st[p].slot * (p ? 4 : 8);
+      budget = 0.4 * ((double)fr + held);
+    }
+    mask = (double)per * 12 <= budget ? 3 : (double)per * 4 <= budget ? 2 : 0;
+  }
+  for (int p = 0; p < 2; p++) {
+    Window::Store &S = W.st[p];
+    S.valid = 0;
+    if (!((mask >> p) & 1)) {
+      window_store_free(p);
+      continue;
+    }
+    if (!S.mem || S.cap < nsteps || S.slot != slot) {
+      window_store_free(p);
+      cuda_check(cudaMalloc(&S.mem, per * (p ? sizeof(float) : sizeof(double))), "cudaMalloc window store");
+      S.cap = nsteps;
+    }
+    S.slot = slot;
+    for (int f = 0; f < 9; f++) S.off[f] = off[f];
+  }
+}
+
 void Engine::window_free_trajectory() {
   Window &W = win;
   graphs_free();
+  window_store_free(0);
+  window_store_free(1);
   for (double *p : W.ck_u) cudaFree(p);
   for (double *p : W.ck_h) cudaFree(p);
   W.ck_u.clear();
@@ -223,16 +303,19 @@ void Engine::window_free_trajectory() {
   W.nsteps = W.every = W.nckpt = 0;
 }
 
-// One nonlinear FP64 step of the window's trajectory from (x_u, x_h) in place.  With `keep`,
-// the four stages' diagnostics and provisional states are left in sd[k] / su[k] (su[0] is the
-// step's start state) and, in precision 1, rounded to FP32.  tl_hook runs after each stage.
+// One nonlinear FP64 step of the window's trajectory from (x_u, x_h) in place.  The four
+// stages' diagnostics and provisional states are left in sd[k] / su[k] (su[0] is the step's
+// start state); in precision 1 their base fields are rounded to FP32 (sd32, su32), and with
+// store_step >= 0 they are written to that step's slots of the valid stores.  hook(k) runs
+// after each stage.
 template <typename Hook>
-static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook) {
+static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook, int store_step = -1) {
   Window &W = E.win;
   const Phys<double> ph = E.phys();
   double w[4], c[4];
   rk_coeffs(ph.dt, w, c);
   double *u0 = W.x_u, *h0 = W.x_h;
+  const bool st64 = store_step >= 0 && W.st[0].mem, st32 = store_step >= 0 && W.st[1].mem;
   for (int k = 0; k < 4; k++) {
     W.su[0] = u0;
     const double *ui = W.su[k];
@@ -242,7 +325,7 @@ static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook) {
     RK<double, double> rh{h0, k == 0 ? h0 : E.acc_h, (k == 3 && in_place) ? h0 : E.acc_h,
                           k < 3 ? W.sh[k + 1] : nullptr, c[k], w[k], 0.0, 0};
     E.fwd_stage(ui, hi, W.sd[k], ph, ru, rh, nullptr, nullptr);
-    if (prec == 1) {
+    if (prec == 1 || st64 || st32) {
       ConvList L{};
       const Diag<double> &d = W.sd[k];
       const Diag<float> &f = W.sd32[k];
@@ -251,7 +334,8 @@ static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook) {
       const long long n[] = {E.nE, E.nE, E.nE, E.nE, E.nE, E.nE, E.nV, E.nV, E.nC};
       for (int i = 0; i < 9; i++) {
         L.src[i] = src[i];
-        L.dst[i] = dst[i];
+        L.dst[i] = st32 ? store_field<float>(W.st[1], store_step, k, i) : prec == 1 ? dst[i] : nullptr;
+        L.dst64[i] = st64 ? store_field<double>(W.st[0], store_step, k, i) : nullptr;
         L.n[i] = n[i];
       }
       L.count = 9;
@@ -267,7 +351,8 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
   Window &W = win;
   const int ev = std::min(every, nsteps), nck = (nsteps + ev - 1) / ev;
   if (W.nsteps && W.every == ev && W.nckpt == nck && W.x_u) {
-    W.nsteps = nsteps;  // same storage layout: reuse every buffer
+    W.nsteps = nsteps;  // same checkpoint layout: reuse every buffer
+    window_store_alloc(nsteps);
     window_trajectory(s);
     return;
   }
@@ -308,72 +393,138 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
     W.su[k] = k == 0 ? nullptr : D(nE);
     W.sh[k] = k == 0 ? nullptr : D(nC);
   }
+  window_store_alloc(nsteps);
   window_trajectory(s);
 }
 
-// Forward over the window from the module's level-1 state, checkpointing.
+// Forward over the window from the module's level-1 state, checkpointing every `every` steps
+// and, when stores are allocated, writing every stage's linearisation point to them (the
+// whole window is then one CUDA graph, since every step writes different slots).
 void Engine::window_trajectory(cudaStream_t s) {
   Window &W = win;
   const int nsteps = W.nsteps;
+  const bool storing = W.st[0].mem || W.st[1].mem;
   cuda_check(cudaStreamSynchronize(s), "window sync");
   cuda_check(cudaMemcpyAsync(W.x_u, dv("u"), sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "copy");
   cuda_check(cudaMemcpyAsync(W.x_h, dv("h"), sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "copy");
-  for (int n = 0; n < nsteps; n++) {
+  auto ckpt = [&](int n) {
     if (n % W.every == 0) {
       cuda_check(cudaMemcpyAsync(W.ck_u[n / W.every], W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "ckpt");
       cuda_check(cudaMemcpyAsync(W.ck_h[n / W.every], W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "ckpt");
     }
-    run_graph(graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(*this, true, 0, [](int) {}); });
+  };
+  if (storing) {
+    GraphKey key = graph_key(6, 0, nsteps, W.st[0].mem, W.st[1].mem);
+    key.n2 = W.every;
+    run_graph(key, [&]() {
+      for (int n = 0; n < nsteps; n++) {
+        ckpt(n);
+        traj_step(*this, true, 0, [](int) {}, n);
+      }
+    });
+  } else {
+    for (int n = 0; n < nsteps; n++) {
+      ckpt(n);
+      run_graph(graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(*this, true, 0, [](int) {}); });
+    }
   }
   cuda_check(cudaMemcpyAsync(W.fin_u, W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "final");
   cuda_check(cudaMemcpyAsync(W.fin_h, W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "final");
   cuda_check(cudaGetLastError(), "window_init");
   cuda_check(cudaStreamSynchronize(stream), "window_init");
+  for (int p = 0; p < 2; p++) W.st[p].valid = W.st[p].mem ? nsteps : 0;
+}
+
+// Member work of tangent-linear stage k about the linearisation point bs.
+template <typename R>
+static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, MemberBufs<R> *mb,
+                            const Phys<R> &ph, const double w[4], const double c[4], int k, const Base<R> &bs) {
+  Window &W = E.win;
+  const MeshDev<R> &m = mesh_for<R>(E);
+  const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
+  const R *hti = k == 0 ? nullptr : mb->ph[k - 1];
+  // stage 1 reads the FP64 member state directly when R is double; otherwise round it
+  if (k == 0) {
+    if constexpr (std::is_same<R, double>::value) {
+      uti = du;
+      hti = dh;
+    } else {
+      convert_d2f((long long)E.nE * B, du, mb->pu[2], E.stream);
+      convert_d2f((long long)E.nC * B, dh, mb->ph[2], E.stream);
+      uti = mb->pu[2];
+      hti = mb->ph[2];
+    }
+  }
+  double *acu = W.ms[prec].acc_u, *ach = W.ms[prec].acc_h;
+  RK<R, double> rut{du, k == 0 ? du : acu, k == 3 ? du : acu, k < 3 ? mb->pu[k] : nullptr, c[k], w[k], R(0), ph.tc1};
+  RK<R, double> rht{dh, k == 0 ? dh : ach, k == 3 ? dh : ach, k < 3 ? mb->ph[k] : nullptr, c[k], w[k], R(0), 0};
+  // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
+  Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, E.stream);
+  Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, E.stream);
+  Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, E.stream);
+  if (ph.visc4 > R(0)) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
+  Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, E.stream);
 }
 
 template <typename R>
 static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
   Window &W = E.win;
   MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
-  const MeshDev<R> &m = mesh_for<R>(E);
   const Phys<double> ph64 = E.phys();
   const Phys<R> ph = phys_as<R>(ph64);
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
-  cuda_check(cudaMemcpyAsync(W.x_u, W.ck_u[0], sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
-  cuda_check(cudaMemcpyAsync(W.x_h, W.ck_h[0], sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
-  auto step = [&]() {
-    traj_step(E, true, prec, [&](int k) {
-      const Base<R> bs = base_for<R>(W, k);
-      const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
-      const R *hti = k == 0 ? nullptr : mb->ph[k - 1];
-      // stage 1 reads the FP64 member state directly when R is double; otherwise round it
-      if (k == 0) {
-        if constexpr (std::is_same<R, double>::value) {
-          uti = du;
-          hti = dh;
-        } else {
-          convert_d2f((long long)E.nE * B, du, mb->pu[2], E.stream);
-          convert_d2f((long long)E.nC * B, dh, mb->ph[2], E.stream);
-          uti = mb->pu[2];
-          hti = mb->ph[2];
-        }
-      }
-      RK<R, double> rut{du, k == 0 ? du : W.ms[prec].acc_u, k == 3 ? du : W.ms[prec].acc_u, k < 3 ? mb->pu[k] : nullptr,
-                        c[k], w[k], R(0), ph.tc1};
-      RK<R, double> rht{dh, k == 0 ? dh : W.ms[prec].acc_h, k == 3 ? dh : W.ms[prec].acc_h, k < 3 ? mb->ph[k] : nullptr,
-                        c[k], w[k], R(0), 0};
-      // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
-      Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, E.stream);
-      Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, E.stream);
-      Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, E.stream);
-      if (ph64.visc4 > 0) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
-      Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, E.stream);
+  if (W.st[prec].valid >= W.nsteps) {
+    // stored linearisation points: the whole sweep is one graph of member kernels
+    GraphKey key = E.graph_key(4, prec, B, du, dh);
+    key.p3 = W.st[prec].mem;
+    key.n2 = W.nsteps;
+    E.run_graph(key, [&]() {
+      for (int n = 0; n < W.nsteps; n++)
+        for (int k = 0; k < 4; k++)
+          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k));
     });
-  };
-  const GraphKey key = E.graph_key(2, prec, B, du, dh);
-  for (int n = 0; n < W.nsteps; n++) E.run_graph(key, step);
+  } else {
+    cuda_check(cudaMemcpyAsync(W.x_u, W.ck_u[0], sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
+    cuda_check(cudaMemcpyAsync(W.x_h, W.ck_h[0], sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
+    // recompute each step's stages; the member work of stage k runs right after stage k (the
+    // FP64 base of stage 1 is the step's start state, which stage 4 overwrites)
+    const GraphKey key = E.graph_key(2, prec, B, du, dh);
+    for (int n = 0; n < W.nsteps; n++)
+      E.run_graph(key, [&]() {
+        traj_step(E, true, prec, [&](int k) { tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, base_for<R>(W, k)); });
+      });
+  }
   cuda_check(cudaGetLastError(), "window_tl");
+}
+
+// Adjoint member work of one step (stages 4..1) about the linearisation points base(k).
+template <typename R, typename BaseOf>
+static void ad_member_step(Engine &E, int prec, int B, double *au, double *ah, MemberBufs<R> *mb,
+                           const Phys<R> &ph, const double w[4], const double c[4], BaseOf &&base) {
+  const MeshDev<R> &m = mesh_for<R>(E);
+  Window::Members &M = E.win.ms[prec];
+  const AdSeeds<R> none{};
+  const double wu4 = ph.tc1 ? 0.0 : w[3];
+  for (int k = 3; k >= 0; k--) {
+    AdIn<R> in{mb->pad_u[(3 - k) & 1], mb->pad_h[(3 - k) & 1]};
+    AdOut<R, double> out{};
+    out.acc_u = M.acc_u; out.acc_h = M.acc_h;
+    out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
+    out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
+    out.tu_next = mb->pad_u[(4 - k) & 1];
+    out.th_next = mb->pad_h[(4 - k) & 1];
+    if (k > 0) {
+      out.wu = ph.tc1 ? 0.0 : w[k - 1];
+      out.cu = ph.tc1 ? 0.0 : c[k - 1];
+      out.wh = w[k - 1];
+      out.ch = c[k - 1];
+    } else {  // stage 4 of the preceding step: tend_ad = w4 * (this step's input adjoint)
+      out.wu = wu4;
+      out.wh = w[3];
+    }
+    Launch<R, double>::ad_stage(m, B, base(k), ph, in, none, mb->w, out, E.stream);
+  }
 }
 
 template <typename R>
@@ -385,12 +536,26 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
   const Phys<R> ph = phys_as<R>(ph64);
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
-  AdSeeds<R> none{};
-  Window::Members &M = W.ms[prec];
   const double wu4 = ph64.tc1 ? 0.0 : w[3];
   // tendency adjoint of the last stage of the last step; later steps get theirs from the
   // final stage of the step after them
-  Launch<R, double>::ad_tinit(m, B, au, ah, nullptr, nullptr, wu4, w[3], mb->pad_u[0], mb->pad_h[0], E.stream);
+  auto tinit = [&]() {
+    Launch<R, double>::ad_tinit(m, B, au, ah, nullptr, nullptr, wu4, w[3], mb->pad_u[0], mb->pad_h[0], E.stream);
+  };
+  if (W.st[prec].valid >= W.nsteps) {
+    // stored linearisation points: the whole sweep is one graph of member kernels
+    GraphKey key = E.graph_key(5, prec, B, au, ah);
+    key.p3 = W.st[prec].mem;
+    key.n2 = W.nsteps;
+    E.run_graph(key, [&]() {
+      tinit();
+      for (int n = W.nsteps - 1; n >= 0; n--)
+        ad_member_step<R>(E, prec, B, au, ah, mb, ph, w, c, [&](int k) { return stored_base<R>(W, prec, n, k); });
+    });
+    cuda_check(cudaGetLastError(), "window_ad");
+    return;
+  }
+  tinit();
   for (int s = W.nckpt - 1; s >= 0; s--) {
     const int first = s * W.every, len = std::min(W.every, W.nsteps - first);
     // replay the segment, keeping the start state of every step
@@ -405,27 +570,9 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
       cuda_check(cudaMemcpyAsync(W.x_u, W.seg_u + (size_t)j * E.nE, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
       cuda_check(cudaMemcpyAsync(W.x_h, W.seg_h + (size_t)j * E.nC, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
       E.run_graph(E.graph_key(3, prec, B, au, ah), [&]() {
-      // forward sweep of this step, keeping the four stages' linearisation points
-      traj_step(E, false, prec, [](int) {});
-      for (int k = 3; k >= 0; k--) {
-        AdIn<R> in{mb->pad_u[(3 - k) & 1], mb->pad_h[(3 - k) & 1]};
-        AdOut<R, double> out{};
-        out.acc_u = M.acc_u; out.acc_h = M.acc_h;
-        out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
-        out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
-        out.tu_next = mb->pad_u[(4 - k) & 1];
-        out.th_next = mb->pad_h[(4 - k) & 1];
-        if (k > 0) {
-          out.wu = ph64.tc1 ? 0.0 : w[k - 1];
-          out.cu = ph64.tc1 ? 0.0 : c[k - 1];
-          out.wh = w[k - 1];
-          out.ch = c[k - 1];
-        } else {  // stage 4 of the preceding step: tend_ad = w4 * (this step's input adjoint)
-          out.wu = wu4;
-          out.wh = w[3];
-        }
-        Launch<R, double>::ad_stage(m, B, base_for<R>(W, k), ph, in, none, mb->w, out, E.stream);
-      }
+        // forward sweep of this step, keeping the four stages' linearisation points
+        traj_step(E, false, prec, [](int) {});
+        ad_member_step<R>(E, prec, B, au, ah, mb, ph, w, c, [&](int k) { return base_for<R>(W, k); });
       });
     }
   }
@@ -525,7 +672,7 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
   const MeshDev<R> &m = mesh_for<R>(E);
   const Phys<double> ph64 = E.phys();
   const Phys<R> ph = phys_as<R>(ph64);
-  const Base<R> bs = base_for<R>(W, 1);
+  const Base<R> bs = W.st[prec].valid ? stored_base<R>(W, prec, 0, 1) : base_for<R>(W, 1);
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
   RK<R, double> rku{W.ms[prec].acc_u, W.ms[prec].acc_u, W.ms[prec].acc_u, mb->pu[1], c[1], w[1], R(0), 0};
@@ -578,6 +725,9 @@ int mpsw_to_internal(mpsw_handle *h, int kind, int B, const double *src, double 
 }
 int mpsw_to_reference(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.to_reference(kind, B, src, dst, (cudaStream_t)stream); });
+}
+int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_storage(mode, max_bytes); });
 }
 int mpsw_window_init(mpsw_handle *h, int nsteps, int ckpt_every, void *stream) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_init(nsteps, ckpt_every, (cudaStream_t)stream); });

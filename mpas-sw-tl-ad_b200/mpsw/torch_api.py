@@ -75,18 +75,25 @@ class Engine:
         return u, h
 
     # ---- windows -------------------------------------------------------------------------
-    def window(self, nsteps: int, ckpt_every: int = 16) -> 'Window':
-        return Window(self, nsteps, ckpt_every)
+    def window(self, nsteps: int, ckpt_every: int = 16, storage: int = -1,
+               max_bytes: float = 0.0) -> 'Window':
+        return Window(self, nsteps, ckpt_every, storage, max_bytes)
 
 
 class Window:
     """``nsteps`` RK4 steps from the engine's current state, checkpointed every
-    ``ckpt_every`` steps; batched tangent-linear and adjoint sweeps over it."""
+    ``ckpt_every`` steps; batched tangent-linear and adjoint sweeps over it.
 
-    def __init__(self, engine: Engine, nsteps: int, ckpt_every: int = 16):
+    ``storage`` selects whether every RK stage's linearisation point is also kept in device
+    memory (``mpsw_window_storage``): -1 automatic (within ``max_bytes``, 0 = 40% of free
+    memory), 0 checkpoints only, 1 FP64, 2 FP32, 3 both.  Results do not depend on it."""
+
+    def __init__(self, engine: Engine, nsteps: int, ckpt_every: int = 16, storage: int = -1,
+                 max_bytes: float = 0.0):
         self.e = engine
         self.nsteps = nsteps
         engine.module.sync()  # pending host-side edits of the module's state first
+        engine.h.call('mpsw_window_storage', int(storage), float(max_bytes))
         engine.h.call('mpsw_window_init', int(nsteps), int(ckpt_every), _stream())
 
     def final_state(self):

@@ -107,3 +107,40 @@ def test_autograd_step_matches_adjoint_and_fd():
     fd = float((jp - jm) / (2 * eps))
     ad = float((u.grad * du).sum() + (h.grad * dh).sum())
     assert abs(fd - ad) / abs(ad) < 1e-6
+
+
+@pytest.mark.parametrize('precision', [0, 1])
+def test_stored_and_recomputed_stages_identical(precision):
+    """Sweeps over stored stage linearisation points equal sweeps that recompute the stages
+    from checkpoints, bit for bit, in both precisions (4 members: vector width 4 in FP32)."""
+    m, e = engine(visc2=1e5, visc4=5e14, drag=True)
+    nsteps, B = 7, 4
+    du, dh = members(m, B, 5)
+    au, ah = members(m, B, 6)
+    out = {}
+    for storage in (0, 3):
+        w = e.window(nsteps, ckpt_every=3, storage=storage)
+        out[storage] = w.tl(du, dh, precision) + w.ad(au, ah, precision)
+    for a, b in zip(out[0], out[3]):
+        assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize('precision', [0, 1])
+def test_member_width_does_not_change_results(precision):
+    """A 4-member sweep (several members per thread) and one-member sweeps (one member per
+    thread) give the same numbers: the per-member arithmetic does not depend on the width."""
+    m, e = engine(visc2=1e5)
+    nsteps, B = 3, 4
+    du, dh = members(m, B, 7)
+    au, ah = members(m, B, 8)
+    w = e.window(nsteps, ckpt_every=2)
+    tu, th = w.tl(du, dh, precision)
+    ru, rh = w.ad(au, ah, precision)
+    for b in range(B):
+        t1 = w.tl(du[:, b:b + 1].contiguous(), dh[:, b:b + 1].contiguous(), precision)
+        r1 = w.ad(au[:, b:b + 1].contiguous(), ah[:, b:b + 1].contiguous(), precision)
+        for x, y in zip(t1 + r1, (tu, th, ru, rh)):
+            if precision == 0:
+                assert torch.equal(x[:, 0], y[:, b])
+            else:  # FP32 stencils are compiled with contraction: allow one rounding per op
+                assert rel(x[:, 0].cpu().numpy(), y[:, b].cpu().numpy()) < 1e-6
