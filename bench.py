@@ -239,6 +239,7 @@ def run_mpsw(a, rank, world):
     import torch
     from module_sw_mpas import MpasSwModule
     from mpsw import _lib
+    from mpsw import replicas
     from mpsw.torch_api import FP32, FP64, Engine, Window
 
     dev = rank % max(1, torch.cuda.device_count())
@@ -253,20 +254,31 @@ def run_mpsw(a, rank, world):
     L = _lib.load()
     B = a.batch
     nC, nE, nV = unit['nCells'], unit['nEdges'], unit['nVertices']
-    dh_h, du_h = perturbations(unit, B, seed=1 + 1000 * rank)
+    dh_h, du_h = perturbations(unit, B, seed=replicas.member_seed(1, rank))
     du = torch.tensor(du_h, device='cuda')
     dh = torch.tensor(dh_h, device='cuda')
     du_i, dh_i = eng.to_internal(du, 1), eng.to_internal(dh, 0)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
 
-    def gradient_batch(prec, Bm, u0, h0):
-        """One bench step on device-resident members: window, TL, AD seeded with the TL output."""
+    def gradient_batch(prec, Bm, u0, h0, ev=None):
+        """One bench step on device-resident members: window, TL, AD seeded with the TL output.
+        With `ev` (four CUDA events) the phase boundaries are recorded on the stream."""
+        rec = (lambda i: ev[i].record(stream)) if ev else (lambda i: None)
+        rec(0)
         w = Window(eng, a.nsteps, a.ckpt, a.storage)
         xu, xh = u0.clone(), h0.clone()
+        rec(1)
         w.tl_internal(xu, xh, prec)
+        rec(2)
         w.ad_internal(xu, xh, prec)
+        rec(3)
         return xu, xh
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
 
     def timed(fn, n_warm, n_time):
         for _ in range(n_warm):
@@ -277,10 +289,12 @@ def run_mpsw(a, rank, world):
             flush.zero_()  # L2 flush between timed iterations, outside the timed region
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
+            barrier()
             e0.record(stream)
             fn()
             e1.record(stream)
             torch.cuda.synchronize()
+            barrier()
             times.append(e0.elapsed_time(e1))
         return times, (L.mpsw_launch_count() - launches0) / n_time
 
@@ -295,13 +309,17 @@ def run_mpsw(a, rank, world):
     with Clocks(dev) as clk:
         t32, launches = timed(lambda: gradient_batch(FP32, B, du_i, dh_i), a.warmup, a.steps)
     clocks = clk.summary()
-    ms = sum(t32) / len(t32)
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], device='cuda', dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    # the job's time is its slowest replica's
+    ms = replicas.max_over_ranks(sum(t32) / len(t32), device='cuda')
     value = world * B / (ms / 1e3)
+
+    # phases of one step (window forward, TL sweep, AD sweep), after an L2 flush
+    flush.zero_()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    gradient_batch(FP32, B, du_i, dh_i, ev)
+    torch.cuda.synchronize()
+    phases = {k: ev[i].elapsed_time(ev[i + 1]) for i, k in enumerate(('window', 'tl', 'ad'))}
 
     # accuracy of the batched FP32 form against the FP64 window on the same members
     ru32, rh32 = gradient_batch(FP32, B, du_i, dh_i)
@@ -380,6 +398,7 @@ def run_mpsw(a, rank, world):
                        'stage_storage': {-1: 'auto (FP64+FP32 stage linearisation points when they fit 40%% of free HBM)', 0: 'none: stages recomputed from checkpoints', 1: 'FP64', 2: 'FP32', 3: 'FP64+FP32'}[a.storage],
                        'members_per_gpu': B, 'parallelism': 'replicas x%d' % world,
                        'l2': 'flushed (256 MB write) between timed steps; working set ~%.0f MB' % wset},
+            'phase_ms': phases,
             'fp64_plain_gradients_per_s': plain,
             'batched_vs_plain': (value / world / plain) if plain else None,
             'rel_err_fp32_vs_fp64': rel_err,
