@@ -15,16 +15,16 @@ int grid_for(long long total) {
 
 void convert_d2f(long long n, const double *src, float *dst, cudaStream_t s) {
   g_launches++;
-  k_convert<double, float><<<LCFG(n), 0, s>>>(n, src, dst);
+  launch_k(k_convert<double, float>, launch_cfg(n), s, n, src, dst);
 }
 void convert_f2d(long long n, const float *src, double *dst, cudaStream_t s) {
   g_launches++;
-  k_convert<float, double><<<LCFG(n), 0, s>>>(n, src, dst);
+  launch_k(k_convert<float, double>, launch_cfg(n), s, n, src, dst);
 }
 
 void convert_list(const ConvList &L, long long max_n, cudaStream_t s) {
   g_launches++;
-  k_convert_list<<<LCFG(max_n), 0, s>>>(L);
+  launch_k(k_convert_list, launch_cfg(max_n), s, L);
 }
 
 template struct Launch<double, double>;

@@ -17,7 +17,18 @@
 
 namespace mpsw {
 
-#define MPSW_GRID_LOOP(t, total)                                                         \
+// Kernels launched with programmatic stream serialisation start while the previous kernel on
+// the stream may still run: wait for it (and its memory writes) before touching any buffer,
+// then let the next kernel be scheduled.  Both are no-ops for a kernel launched without it.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Grid-stride loop over `total` work items, preceded by pdl_begin(): every kernel body starts
+// with it.
+#define MPSW_GRID_LOOP(t, total)                                                               \
+  pdl_begin();                                                                                 \
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)(total); \
        t += (long long)gridDim.x * blockDim.x)
 
@@ -299,6 +310,7 @@ __global__ void k_convert(long long n, const S *__restrict__ src, D *dst) {
 
 // Rounds up to kConvMax double arrays to float in one launch (linearisation point of a stage).
 static __global__ void k_convert_list(ConvList L) {
+  pdl_begin();  // also when the list is empty
   for (int i = 0; i < L.count; i++) {
     const double *__restrict__ s = L.src[i];
     float *__restrict__ d = L.dst[i];

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <initializer_list>
+#include <utility>
 
 #include "mpsw_kernels.cuh"
 #include "mpsw_launch.h"
@@ -27,7 +28,32 @@ inline LaunchCfg launch_cfg(long long total) {
   if (g < 1) g = 1;
   return {(int)(g < cap ? g : cap), block};
 }
-#define LCFG(total) launch_cfg(total).grid, launch_cfg(total).block
+
+// Programmatic dependent launch: every kernel is launched with programmatic stream
+// serialisation, so the GPU may schedule it while its predecessor on the stream is still
+// draining; each kernel begins with griddepcontrol.wait (pdl_begin, in MPSW_GRID_LOOP), which
+// returns once the predecessor has completed and its writes are visible.  MPSW_PDL=0 launches
+// with plain stream order instead.
+inline bool pdl_enabled() {
+  static const bool on = !(std::getenv("MPSW_PDL") && std::atoi(std::getenv("MPSW_PDL")) == 0);
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), LaunchCfg c, cudaStream_t s, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)c.grid);
+  cfg.blockDim = dim3((unsigned)c.block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  // a failed launch is reported by the cudaGetLastError check that follows every launch sequence
+  (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // every kernel launch of the engine goes through one of these launchers and is counted here
 extern long long g_launches;
@@ -61,56 +87,55 @@ inline int vec_width(int B, std::initializer_list<const void *> ptrs) {
     case 2: { constexpr int VV = 2; __VA_ARGS__; } break;  \
     default: { constexpr int VV = 1; __VA_ARGS__; } break; \
   }
-#define LCFGV(n, B, v) LCFG((long long)(n) * ((B) / (v)))
 
 template <typename R, typename A>
 void Launch<R, A>::fwd_vertex(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                               cudaStream_t s) {
   g_launches++;
-  k_fwd_vertex<R><<<LCFG(m.nV), 0, s>>>(m, u, h, off, d);
+  launch_k(k_fwd_vertex<R>, launch_cfg(m.nV), s, m, u, h, off, d);
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_cell(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                             const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
-  k_fwd_cell<R, A><<<LCFG(m.nC), 0, s>>>(m, u, h, off, d, rk, tend_h);
+  launch_k(k_fwd_cell<R, A>, launch_cfg(m.nC), s, m, u, h, off, d, rk, tend_h);
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                                  const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
-  k_fwd_edge_diag<R><<<LCFG(m.nE), 0, s>>>(m, u, h, off, d, ph);
+  launch_k(k_fwd_edge_diag<R>, launch_cfg(m.nE), s, m, u, h, off, d, ph);
 }
 template <typename R, typename A>
 void Launch<R, A>::del4_vc(const MeshDev<R> &m, int B, const R *dsq_u, R *dsq_vort, R *dsq_div,
                            cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {dsq_u, dsq_vort, dsq_div});
-  MPSW_VDISPATCH(v, (k_del4_vc<R, VV><<<LCFGV(m.nV + m.nC, B, VV), 0, s>>>(m, B, dsq_u, dsq_vort, dsq_div)));
+  MPSW_VDISPATCH(v, (launch_k(k_del4_vc<R, VV>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (VV))), s, m, B, dsq_u, dsq_vort, dsq_div)));
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                                  const Phys<R> &ph, const RK<R, A> &rk, R *tend_u, cudaStream_t s) {
   g_launches++;
-  k_fwd_edge_tend<R, A><<<LCFG(m.nE), 0, s>>>(m, u, h, off, d, ph, rk, tend_u);
+  launch_k(k_fwd_edge_tend<R, A>, launch_cfg(m.nE), s, m, u, h, off, d, ph, rk, tend_u);
 }
 template <typename R, typename A>
 void Launch<R, A>::tend_h(const MeshDev<R> &m, const R *u, const R *he, R *out, cudaStream_t s) {
   g_launches++;
-  k_tend_h<R><<<LCFG(m.nC), 0, s>>>(m, u, he, out);
+  launch_k(k_tend_h<R>, launch_cfg(m.nC), s, m, u, he, out);
 }
 template <typename R, typename A>
 void Launch<R, A>::recon(const MeshDev<R> &m, int B, int sphere, const R *u, R *X, R *Y, R *Z, R *Zon,
                          R *Mer, cudaStream_t s) {
   g_launches++;
-  k_recon<R><<<LCFG((long long)m.nC * B), 0, s>>>(m, B, sphere, u, X, Y, Z, Zon, Mer);
+  launch_k(k_recon<R>, launch_cfg((long long)m.nC * B), s, m, B, sphere, u, X, Y, Z, Zon, Mer);
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                              const Diag<R> &d, cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.circ, d.vort, d.hv, d.pvv});
-  MPSW_VDISPATCH(v, (k_tl_vertex<R, VV><<<LCFGV(m.nV, B, VV), 0, s>>>(m, B, bs, ut, ht, d)));
+  MPSW_VDISPATCH(v, (launch_k(k_tl_vertex<R, VV>, launch_cfg((long long)(m.nV) * ((B) / (VV))), s, m, B, bs, ut, ht, d)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
@@ -118,14 +143,14 @@ void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const 
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.div, d.ke, d.pc, d.vc, d.pvv, d.vort, tend_h, rk.x0, rk.acc_in,
                                     rk.acc_out, rk.next});
-  MPSW_VDISPATCH(v, (k_tl_cell<R, A, VV><<<LCFGV(m.nC, B, VV), 0, s>>>(m, B, bs, ut, ht, d, rk, tend_h)));
+  MPSW_VDISPATCH(v, (launch_k(k_tl_cell<R, A, VV>, launch_cfg((long long)(m.nC) * ((B) / (VV))), s, m, B, bs, ut, ht, d, rk, tend_h)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                                 const Diag<R> &d, const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.pvv, d.pc, d.div, d.vort, d.pe, d.he, d.v, d.gpt, d.gpn, d.dsq_u});
-  MPSW_VDISPATCH(v, (k_tl_edge_diag<R, VV><<<LCFGV(m.nE, B, VV), 0, s>>>(m, B, bs, ut, ht, d, ph)));
+  MPSW_VDISPATCH(v, (launch_k(k_tl_edge_diag<R, VV>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, d, ph)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
@@ -134,7 +159,7 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
                                     rk.x0, rk.acc_in, rk.acc_out, rk.next});
-  MPSW_VDISPATCH(v, (k_tl_edge_tend<R, A, VV><<<LCFGV(m.nE, B, VV), 0, s>>>(m, B, bs, ut, ht, d, ph, rk, tend_u)));
+  MPSW_VDISPATCH(v, (launch_k(k_tl_edge_tend<R, A, VV>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, d, ph, rk, tend_u)));
 }
 // members per thread of one adjoint stage: every buffer the five kernels touch
 template <typename R, typename A>
@@ -150,12 +175,12 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
                       cudaStream_t s) {
   g_launches++;
   switch (which) {
-    case 0: k_ad_edge<R, A, V><<<LCFGV(m.nE, B, V), 0, s>>>(m, B, bs, ph, in, sd, w); break;
-    case 1: k_ad_cell<R, A, V><<<LCFGV(m.nC, B, V), 0, s>>>(m, B, bs, ph, in, sd, w); break;
-    case 2: k_ad_vertex<R, A, V><<<LCFGV(m.nV, B, V), 0, s>>>(m, B, bs, ph, in, sd, w); break;
-    case 3: k_ad_final<R, A, V><<<LCFGV(m.nC + m.nE, B, V), 0, s>>>(m, B, bs, w, out); break;
-    case 4: k_ad_del4_vc<R, V><<<LCFGV(m.nV + m.nC, B, V), 0, s>>>(m, B, ph, in, w); break;
-    default: k_ad_del4_e<R, V><<<LCFGV(m.nE, B, V), 0, s>>>(m, B, w); break;
+    case 0: launch_k(k_ad_edge<R, A, V>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
+    case 1: launch_k(k_ad_cell<R, A, V>, launch_cfg((long long)(m.nC) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
+    case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
+    case 3: launch_k(k_ad_final<R, A, V>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V))), s, m, B, bs, w, out); break;
+    case 4: launch_k(k_ad_del4_vc<R, V>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (V))), s, m, B, ph, in, w); break;
+    default: launch_k(k_ad_del4_e<R, V>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, w); break;
   }
 }
 
@@ -188,36 +213,36 @@ void Launch<R, A>::ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x
                             const R *seed_th, A wu, A wh, R *tu, R *th, cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {x2u, x2h, tu, th});
-  MPSW_VDISPATCH(v, (k_ad_tinit<R, A, VV><<<LCFGV(m.nE + m.nC, B, VV), 0, s>>>(m, B, x2u, x2h, seed_tu, seed_th,
+  MPSW_VDISPATCH(v, (launch_k(k_ad_tinit<R, A, VV>, launch_cfg((long long)(m.nE + m.nC) * ((B) / (VV))), s, m, B, x2u, x2h, seed_tu, seed_th,
                                                                                 wu, wh, tu, th)));
 }
 template <typename R, typename A>
 void Launch<R, A>::recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea,
                              A *u_ad, cudaStream_t s) {
   g_launches++;
-  k_recon_adj_cell<R><<<LCFG(m.nC), 0, s>>>(m, sphere, Xa, Ya, Za, Zoa, Mea);
+  launch_k(k_recon_adj_cell<R>, launch_cfg(m.nC), s, m, sphere, Xa, Ya, Za, Zoa, Mea);
   g_launches++;
-  k_recon_adj_edge<R, A><<<LCFG(m.nE), 0, s>>>(m, Xa, Ya, Za, u_ad);
+  launch_k(k_recon_adj_edge<R, A>, launch_cfg(m.nE), s, m, Xa, Ya, Za, u_ad);
 }
 template <typename R, typename A>
 void Launch<R, A>::to_internal(int n, int B, const int *perm, const double *src, R *dst, cudaStream_t s) {
   g_launches++;
-  k_to_internal<double, R><<<LCFG((long long)n * B), 0, s>>>(n, B, perm, src, dst);
+  launch_k(k_to_internal<double, R>, launch_cfg((long long)n * B), s, n, B, perm, src, dst);
 }
 template <typename R, typename A>
 void Launch<R, A>::to_reference(int n, int B, const int *perm, const R *src, double *dst, cudaStream_t s) {
   g_launches++;
-  k_to_reference<R, double><<<LCFG((long long)n * B), 0, s>>>(n, B, perm, src, dst);
+  launch_k(k_to_reference<R, double>, launch_cfg((long long)n * B), s, n, B, perm, src, dst);
 }
 template <typename R, typename A>
 void Launch<R, A>::to_internal_acc(int n, int B, const int *perm, const double *src, A *dst, cudaStream_t s) {
   g_launches++;
-  k_to_internal<double, A><<<LCFG((long long)n * B), 0, s>>>(n, B, perm, src, dst);
+  launch_k(k_to_internal<double, A>, launch_cfg((long long)n * B), s, n, B, perm, src, dst);
 }
 template <typename R, typename A>
 void Launch<R, A>::to_reference_acc(int n, int B, const int *perm, const A *src, double *dst, cudaStream_t s) {
   g_launches++;
-  k_to_reference<A, double><<<LCFG((long long)n * B), 0, s>>>(n, B, perm, src, dst);
+  launch_k(k_to_reference<A, double>, launch_cfg((long long)n * B), s, n, B, perm, src, dst);
 }
 
 }  // namespace mpsw
