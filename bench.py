@@ -28,7 +28,7 @@ sys.path.insert(0, os.path.join(ROOT, 'mpas-sw-tl-ad_b200'))
 METRIC = 'TL+AD gradients/s, batched FP32 vs plain FP64 (rel err<=1e-4)'
 UNIT = 'gradients/s'
 KERNELS = ['tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend', 'ad_edge', 'ad_cell',
-           'ad_vertex', 'ad_final']
+           'ad_vertex', 'ad_final', 'tl_stage', 'ad_stage']
 
 
 def parse():
@@ -45,6 +45,9 @@ def parse():
     p.add_argument('--storage', type=int, default=-1,
                    help='stage storage mode of the window: -1 auto, 0 checkpoints only, 1 FP64, 2 FP32, 3 both')
     p.add_argument('--no-plain', action='store_true', help='skip the plain FP64 arm')
+    p.add_argument('--profile-kernels', action='store_true',
+                   help='one small window, then each member kernel once (twice with its warm-up) inside '
+                        'the NVTX range "mpsw_kernels", as mpsw_time_kernel launches them; no JSON line')
     p.add_argument('--profile', action='store_true',
                    help='only the timed batched windows (for profiler launch lists); no JSON line')
     return p.parse_args()
@@ -216,22 +219,56 @@ class Clocks:
 
 # ---- algorithmic bytes of the member kernels ------------------------------------------------------
 def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
-    """Bytes a launch must move if every array element it touches is read or written once.
-    s: bytes of a member / linearisation-point value (8 or 4); accumulators are 8 bytes;
-    connectivity words 4 bytes, mesh metrics s bytes."""
-    a = 8
-    mesh_e = 4 * (nE + sum_eoe) + s * sum_eoe          # nEdgesOnEdge, edgesOnEdge, weights
-    if name == 'tl_edge_tend':
-        mesh = mesh_e + 4 * 4 * nE + 2 * s * nE        # c1,c2,v1,v2; dc,dv
-        base = 3 * s * nE                               # pv_edge, u, h_edge
-        mem = B * (3 * s * nE + 2 * s * nC + 3 * a * nE + s * nE)  # u,pe,he,h,ke; x0,acc r/w; next
-        return mesh + base + mem
-    if name == 'ad_edge':
-        mesh = mesh_e + 4 * sum_eoe + 2 * 4 * nE + s * nE + s * nC   # rev; c1,c2; dv; area
-        base = 6 * s * nE                               # u, h_edge, pv_edge, gradPVn, gradPVt, v
-        mem = B * ((2 * a + s) * nE + (2 * a + s) * nC + 6 * s * nE)  # x2 + next pad (u,h); 6 outputs
-        return mesh + base + mem
-    raise KeyError(name)
+    """Bytes a launch must move if every array element it touches is read or written once
+    (viscosity, drag and wind off, as in the benchmark workload).
+
+    s: bytes of a member value, a linearisation-point value and a mesh metric (4 in FP32);
+    accumulators and member RK states are a = 8 bytes; connectivity words 4 bytes, edge signs
+    1 byte.  E, C, V: edges, cells, vertices.  As mpsw_time_kernel launches them, the RK state
+    x0 and the accumulator are one FP64 array, so RK bookkeeping reads it, writes it and writes
+    the next provisional state (2a + s per member value); ad_final's x2 is that array too."""
+    a, i, E, C, V, S = 8, 4, nE, nC, nV, sum_eoe
+    eoe = i * (E + S) + s * S                              # nEdgesOnEdge, edgesOnEdge, weights
+    kb = {
+        'tl_vertex': (3 * i + 3 + 3 * i + 3 * s) * V + 2 * s * V + s * E   # v_es,esg,v_c,kites; area,f; dc
+                     + 2 * s * V                                          # base h_vertex, vorticity
+                     + B * s * (E + C + 2 * V),                           # u,h in; vort, pv out
+        'tl_cell': (i + 3 * 6 * i + 6 + 6 * s + s) * C + (2 * i + 2 * s) * E  # c_n,es,eoc,vs,esg,kites,area; c1,c2,dc,dv
+                   + 2 * s * E                                                  # base u, h_edge
+                   + B * (s * (E + C + V + 3 * C) + (2 * a + s) * C),          # u,h,pv in; div,ke,pc out; RK
+        'tl_edge_diag': eoe + (6 * i + 2 * s) * E + 4 * s * E                  # ends; dc,dv; base gradPVt,v,gradPVn,u
+                        + B * s * (E + C + V + C + 2 * E),                     # u,h,pv,pc in; pv_edge,h_edge out
+        'tl_edge_tend': eoe + (2 * i + s) * E + 3 * s * E                      # c1,c2,dc; base pv_edge,u,h_edge
+                        + B * (s * (3 * E + 2 * C) + (2 * a + s) * E),         # u,pe,he,ke,h in; RK
+        'ad_edge': eoe + s * S + (2 * i + s) * E + 6 * s * E                   # wrev; c1,c2,dv; 6 base fields
+                   + B * s * (E + C + 6 * E),                                  # tu,th in; 6 adjoints out
+        'ad_cell': (i + 6 * i + 6 + s) * C + s * E                             # c_n,es,esg,area; dc
+                   + B * s * (3 * E + 4 * C),                                  # tu,gpn_ad,he_ad in; 4 out
+        'ad_vertex': (3 * i + 3 * s + 3 * i + 3 * i + 3 + 2 * s) * V + s * C + s * E + 2 * s * V
+                     + B * s * (C + 2 * E + 2 * V),                            # pc_ad,pe_ad,gpt_ad in; 2 out
+        'ad_final': (i + 6 * i + 6 * s + s) * C + i * (E + S) + s * S + (4 * i + 2 * s) * E + s * E
+                    + B * (s * (2 * C + 2 * V + 2 * E + C) + (2 * a + s) * (C + E)),
+    }
+    kb['tl_stage'] = sum(kb[k] for k in ('tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend'))
+    kb['ad_stage'] = sum(kb[k] for k in ('ad_edge', 'ad_cell', 'ad_vertex', 'ad_final'))
+    return kb[name]
+
+
+def traffic_of(kernel, level, B):
+    """DRAM bytes (read + write) of one launch of `kernel`, from the committed ncu summary of
+    that kernel on this workload (profiles/k_<kernel>_l<level>_b<B>_fp32.md), or None."""
+    import re
+    path = os.path.join(ROOT, 'profiles', 'k_%s_l%d_b%d_fp32.md' % (kernel, level, B))
+    if not os.path.exists(path):
+        return None
+    unit = {'byte': 1, 'Kbyte': 1e3, 'Mbyte': 1e6, 'Gbyte': 1e9}
+    total, found = 0.0, 0
+    for line in open(path):
+        m = re.search(r'dram__bytes_(read|write)\.sum`?\)?\s*\|\s*([0-9.]+)\s*(\w+)', line)
+        if m and m.group(3) in unit:
+            total += float(m.group(2)) * unit[m.group(3)]
+            found += 1
+    return total if found == 2 else None
 
 
 def run_mpsw(a, rank, world):
@@ -303,6 +340,16 @@ def run_mpsw(a, rank, world):
         dist.barrier()
 
     # batched FP32 stencils / FP64 accumulation: the headline
+    if a.profile_kernels:
+        import ctypes
+        gradient_batch(FP32, B, du_i, dh_i)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push('mpsw_kernels')
+        for i in range(len(KERNELS) - 2):
+            out = ctypes.c_double()
+            eng.h.check(L.mpsw_time_kernel(eng.h.ptr, i, FP32, B, 1, ctypes.byref(out)), 'time_kernel')
+        torch.cuda.nvtx.range_pop()
+        return
     if a.profile:
         timed(lambda: gradient_batch(FP32, B, du_i, dh_i), a.warmup, a.steps)
         return
@@ -371,13 +418,17 @@ def run_mpsw(a, rank, world):
         out = ctypes.c_double()
         eng.h.check(L.mpsw_time_kernel(eng.h.ptr, i, FP32, B, 20, ctypes.byref(out)), 'time_kernel')
         kt[name] = out.value
-    top = max(('tl_edge_tend', 'ad_edge'), key=lambda k: kt[k])
+    # every member kernel launches once per stage: the dominant one is the slowest
+    top = max(KERNELS[:8], key=lambda k: kt[k])
     bytes_ = kernel_bytes(top, nC, nE, nV, sum_eoe, B, 4)
     ach = bytes_ / (kt[top] / 1e3) / 1e9
+    stages = {k: {'ms': kt[k], 'algorithmic_bytes': kernel_bytes(k, nC, nE, nV, sum_eoe, B, 4),
+                  'achieved_gbs': kernel_bytes(k, nC, nE, nV, sum_eoe, B, 4) / (kt[k] / 1e3) / 1e9}
+              for k in ('tl_stage', 'ad_stage')}
     roof = {'bound': 'hbm', 'kernel': top, 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
-            'frac': ach / hbm, 'peak_source': peak_kind, 'traffic': None,
+            'frac': ach / hbm, 'peak_source': peak_kind, 'traffic': traffic_of(top, a.level, B),
             'algorithmic_bytes': bytes_, 'ms_per_launch': kt[top],
-            'kernel_ms': kt}
+            'kernel_ms': {k: kt[k] for k in KERNELS[:8]}, 'stages': stages}
 
     # host baseline: serial oracle on one core, bounded sample
     cpu = None

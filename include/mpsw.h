@@ -139,8 +139,9 @@ int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const double *hh,
 long long mpsw_launch_count(void);
 /* Average time of `iters` back-to-back launches of one member stencil kernel on the buffers
  * of the last window sweep (same precision and B): which = 0 tl_vertex, 1 tl_cell,
- * 2 tl_edge_diag, 3 tl_edge_tend, 4 ad_edge, 5 ad_cell, 6 ad_vertex, 7 ad_final.  Timed with
- * CUDA events on the engine's stream. */
+ * 2 tl_edge_diag, 3 tl_edge_tend, 4 ad_edge, 5 ad_cell, 6 ad_vertex, 7 ad_final; or of a whole
+ * stage: 8 tangent-linear stage, 9 adjoint stage.  Timed with CUDA events on the engine's
+ * stream. */
 int mpsw_time_kernel(mpsw_handle *h, int which, int precision, int B, int iters, double *ms_per_launch);
 
 #ifdef __cplusplus

@@ -339,6 +339,8 @@ void Engine::fill_mesh(MeshDev<R> &m) {
   m.nC = bm.nC;
   m.nE = bm.nE;
   m.nV = bm.nV;
+  m.max_eoe = bm.e_n.empty() ? 0 : *std::max_element(bm.e_n.begin(), bm.e_n.end());
+  m.max_eoc = bm.c_n.empty() ? 0 : *std::max_element(bm.c_n.begin(), bm.c_n.end());
   m.c_n = up<int>(bm.c_n, o);
   m.c_eoc = up<int>(bm.c_eoc, o);
   m.c_es = up<int>(bm.c_es, o);

@@ -31,6 +31,7 @@ constexpr double RHO_REF = 1000.0;
 template <typename R>
 struct MeshDev {
   int nC, nE, nV;
+  int max_eoe, max_eoc;        // largest nEdgesOnEdge and nEdgesOnCell of the mesh
   // cells
   const int *c_n;              // [N]      nEdgesOnCell
   const int *c_eoc;            // [MAXE][N] edgesOnCell, reference slot order

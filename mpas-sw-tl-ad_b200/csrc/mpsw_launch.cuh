@@ -19,6 +19,7 @@ constexpr int kThreads = 256;
 // fewer than two blocks per SM, so thin single-trajectory launches still spread over all SMs.
 struct LaunchCfg {
   int grid, block;
+  size_t smem = 0;  // dynamic shared memory bytes
 };
 inline LaunchCfg launch_cfg(long long total) {
   int block = kThreads;
@@ -26,7 +27,7 @@ inline LaunchCfg launch_cfg(long long total) {
   long long g = (total + block - 1) / block;
   const long long cap = 148LL * 16 * (kThreads / block);
   if (g < 1) g = 1;
-  return {(int)(g < cap ? g : cap), block};
+  return {(int)(g < cap ? g : cap), block, 0};
 }
 
 // Programmatic dependent launch: every kernel is launched with programmatic stream
@@ -44,7 +45,7 @@ inline void launch_k(void (*kernel)(KArgs...), LaunchCfg c, cudaStream_t s, Args
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)c.grid);
   cfg.blockDim = dim3((unsigned)c.block);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = c.smem;
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -81,6 +82,34 @@ inline int vec_width(int B, std::initializer_list<const void *> ptrs) {
 }
 
 // run the statement with the compile-time member width VV equal to the runtime width v
+// Staged edge kernels: blocks of epb = 256 / (B / V) edges (B / V threads each), used when the
+// mesh has narrow bounds and a block holds at least two edges.  MPSW_STAGE=0 disables them.
+inline bool stage_enabled() {
+  static const bool on = !(std::getenv("MPSW_STAGE") && std::atoi(std::getenv("MPSW_STAGE")) == 0);
+  return on;
+}
+// (and the block's stage fits the default 48 KB of dynamic shared memory)
+template <typename R>
+inline bool use_staged(const MeshDev<R> &m, int B, int v, size_t smem_per_edge_bytes) {
+  const int tpe = B / v;
+  return stage_enabled() && m.max_eoe <= BoundsNarrow::e2 && m.max_eoc <= BoundsNarrow::c && tpe <= 128 &&
+         smem_per_edge_bytes * (kThreads / tpe) <= 48 * 1024;
+}
+inline LaunchCfg staged_cfg(int n, int B, int v, size_t smem_per_edge_bytes) {
+  const int tpe = B / v, epb = kThreads / tpe;
+  return {(n + epb - 1) / epb, epb * tpe, smem_per_edge_bytes * epb};
+}
+
+// run the statement with NB = BoundsNarrow when the mesh allows it, else BoundsAny
+#define MPSW_BDISPATCH(m, ...)                                  \
+  if ((m).max_eoe <= BoundsNarrow::e2 && (m).max_eoc <= BoundsNarrow::c) { \
+    using NB = BoundsNarrow;                                    \
+    __VA_ARGS__;                                                \
+  } else {                                                      \
+    using NB = BoundsAny;                                       \
+    __VA_ARGS__;                                                \
+  }
+
 #define MPSW_VDISPATCH(v, ...)                            \
   switch (v) {                                            \
     case 4: { constexpr int VV = 4; __VA_ARGS__; } break;  \
@@ -104,14 +133,16 @@ template <typename R, typename A>
 void Launch<R, A>::fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                                  const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
-  launch_k(k_fwd_edge_diag<R>, launch_cfg(m.nE), s, m, u, h, off, d, ph);
+  Diag<R> dd = d;
+  if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
+  launch_k(k_fwd_edge_diag<R>, launch_cfg(m.nE), s, m, u, h, off, dd, ph);
 }
 template <typename R, typename A>
 void Launch<R, A>::del4_vc(const MeshDev<R> &m, int B, const R *dsq_u, R *dsq_vort, R *dsq_div,
                            cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {dsq_u, dsq_vort, dsq_div});
-  MPSW_VDISPATCH(v, (launch_k(k_del4_vc<R, VV>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (VV))), s, m, B, dsq_u, dsq_vort, dsq_div)));
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_del4_vc<R, VV, NB>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (VV))), s, m, B, dsq_u, dsq_vort, dsq_div)));
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
@@ -143,14 +174,16 @@ void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const 
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.div, d.ke, d.pc, d.vc, d.pvv, d.vort, tend_h, rk.x0, rk.acc_in,
                                     rk.acc_out, rk.next});
-  MPSW_VDISPATCH(v, (launch_k(k_tl_cell<R, A, VV>, launch_cfg((long long)(m.nC) * ((B) / (VV))), s, m, B, bs, ut, ht, d, rk, tend_h)));
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_cell<R, A, VV, NB>, launch_cfg((long long)(m.nC) * ((B) / (VV))), s, m, B, bs, ut, ht, d, rk, tend_h)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                                 const Diag<R> &d, const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
-  const int v = vec_width<R, A>(B, {ut, ht, d.pvv, d.pc, d.div, d.vort, d.pe, d.he, d.v, d.gpt, d.gpn, d.dsq_u});
-  MPSW_VDISPATCH(v, (launch_k(k_tl_edge_diag<R, VV>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, d, ph)));
+  Diag<R> dd = d;
+  if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
+  const int v = vec_width<R, A>(B, {ut, ht, dd.pvv, dd.pc, dd.div, dd.vort, dd.pe, dd.he, dd.v, dd.gpt, dd.gpn, dd.dsq_u});
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, dd, ph)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
@@ -159,7 +192,13 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
                                     rk.x0, rk.acc_in, rk.acc_out, rk.next});
-  MPSW_VDISPATCH(v, (launch_k(k_tl_edge_tend<R, A, VV>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, d, ph, rk, tend_u)));
+  constexpr int J = BoundsNarrow::e2;
+  if (use_staged(m, B, v, eoe_stage_bytes<R, J, 3>(1))) {
+    MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eoe_stage_bytes<R, J, 3>(1)),
+                               s, m, B, bs, ut, ht, d, ph, rk, tend_u));
+    return;
+  }
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_tend<R, A, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, d, ph, rk, tend_u)));
 }
 // members per thread of one adjoint stage: every buffer the five kernels touch
 template <typename R, typename A>
@@ -169,17 +208,17 @@ static int ad_width(int B, const AdIn<R> &in, const AdWork<R> &w, const AdOut<R,
                              out.x2u, out.x2h, out.dst_u, out.dst_h, out.tu_next, out.th_next});
 }
 
-template <typename R, typename A, int V>
+template <typename R, typename A, int V, class NB>
 static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                       const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w, const AdOut<R, A> &out,
                       cudaStream_t s) {
   g_launches++;
   switch (which) {
-    case 0: launch_k(k_ad_edge<R, A, V>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
-    case 1: launch_k(k_ad_cell<R, A, V>, launch_cfg((long long)(m.nC) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
+    case 0: launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
+    case 1: launch_k(k_ad_cell<R, A, V, NB>, launch_cfg((long long)(m.nC) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
     case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
-    case 3: launch_k(k_ad_final<R, A, V>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V))), s, m, B, bs, w, out); break;
-    case 4: launch_k(k_ad_del4_vc<R, V>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (V))), s, m, B, ph, in, w); break;
+    case 3: launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V))), s, m, B, bs, w, out); break;
+    case 4: launch_k(k_ad_del4_vc<R, V, NB>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (V))), s, m, B, ph, in, w); break;
     default: launch_k(k_ad_del4_e<R, V>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, w); break;
   }
 }
@@ -189,16 +228,16 @@ void Launch<R, A>::ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const
                             const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
                             const AdOut<R, A> &out, cudaStream_t s) {
   const int v = ad_width<R, A>(B, in, w, out);
-  MPSW_VDISPATCH(v, {
-    ad_launch<R, A, VV>(0, m, B, bs, ph, in, sd, w, out, s);
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, {
+    ad_launch<R, A, VV, NB>(0, m, B, bs, ph, in, sd, w, out, s);
     if (ph.visc4 > R(0)) {
-      ad_launch<R, A, VV>(4, m, B, bs, ph, in, sd, w, out, s);
-      ad_launch<R, A, VV>(5, m, B, bs, ph, in, sd, w, out, s);
+      ad_launch<R, A, VV, NB>(4, m, B, bs, ph, in, sd, w, out, s);
+      ad_launch<R, A, VV, NB>(5, m, B, bs, ph, in, sd, w, out, s);
     }
-    ad_launch<R, A, VV>(1, m, B, bs, ph, in, sd, w, out, s);
-    ad_launch<R, A, VV>(2, m, B, bs, ph, in, sd, w, out, s);
-    ad_launch<R, A, VV>(3, m, B, bs, ph, in, sd, w, out, s);
-  });
+    ad_launch<R, A, VV, NB>(1, m, B, bs, ph, in, sd, w, out, s);
+    ad_launch<R, A, VV, NB>(2, m, B, bs, ph, in, sd, w, out, s);
+    ad_launch<R, A, VV, NB>(3, m, B, bs, ph, in, sd, w, out, s);
+  }));
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
@@ -206,7 +245,7 @@ void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> 
                            cudaStream_t s) {
   const AdSeeds<R> sd{};
   const int v = ad_width<R, A>(B, in, w, out);
-  MPSW_VDISPATCH(v, (ad_launch<R, A, VV>(which < 0 || which > 3 ? 3 : which, m, B, bs, ph, in, sd, w, out, s)));
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(which < 0 || which > 3 ? 3 : which, m, B, bs, ph, in, sd, w, out, s)));
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,

@@ -90,6 +90,23 @@ __device__ __forceinline__ EntMember ent_member(long long t, int B, int V) {
   return {ent, (int)(t - (long long)ent * bv) * V};
 }
 
+// Bounds of the neighbour loops.  BoundsNarrow serves meshes with at most 10 edgesOnEdge and 6
+// edgesOnCell (every quasi-uniform hexagon/pentagon mesh): the loops get compile-time trip
+// counts and are unrolled with `slot < n` as a predicate, so the connectivity, weight and member
+// loads of all slots can be in flight together instead of one slot after another.  BoundsAny
+// keeps runtime trip counts for any mesh within MAXE2 / MAXE.
+struct BoundsNarrow {
+  static constexpr int e2 = 10, c = 6;
+};
+struct BoundsAny {
+  static constexpr int e2 = 0, c = 0;
+};
+
+// j over the first n slots of a list whose length is at most NMAX (NMAX 0: no static bound)
+#define MPSW_SLOTS(j, NMAX, n)                                                \
+  _Pragma("unroll") for (int j = 0; j < ((NMAX) > 0 ? (NMAX) : (n)); j++) \
+    if ((NMAX) == 0 || j < (n))
+
 // RK4 bookkeeping of V members (src/mpas_sw_module.f90:590-611)
 template <typename R, typename A, int V>
 __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const Mv<R, V> &t) {
@@ -110,7 +127,7 @@ __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const M
 
 // del4 intermediates (src/mpas_sw_dyncore.f90:554-589): delsq_vorticity on vertices and
 // delsq_divergence on cells.  One grid covers the vertex threads followed by the cell threads.
-template <typename R, int V>
+template <typename R, int V, class NB>
 __global__ void k_del4_vc(MeshDev<R> m, int B, const R *__restrict__ dsq_u, R *dsq_vort, R *dsq_div) {
   using M = Mv<R, V>;
   const int nV = m.nV, nC = m.nC;
@@ -132,7 +149,7 @@ __global__ void k_del4_vc(MeshDev<R> m, int B, const R *__restrict__ dsq_u, R *d
       const int c = q.ent;
       const int n = ld(m.c_n, c);
       M dd = mv_fill<R, V>(R(0));
-      for (int k = 0; k < n; k++) {
+      MPSW_SLOTS(k, NB::c, n) {
         const int e = ld(m.c_es, (size_t)k * nC + c);
         const R s = R(m.c_esg[(size_t)k * nC + c]);
         dd = dd + s * (ldv<V>(dsq_u + (size_t)e * B + q.b) * ld(m.e_dv, e));
@@ -180,7 +197,7 @@ __global__ void k_tl_vertex(MeshDev<R> m, int B, Base<R> bs, const R *__restrict
 }
 
 // :274-316, :397-421, thickness tendency :541-561 and the RK update
-template <typename R, typename A, int V>
+template <typename R, typename A, int V, class NB>
 __global__ void k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                           const R *__restrict__ ht, Diag<R> d, RK<R, A> rk, R *tend_h) {
   using M = Mv<R, V>;
@@ -190,7 +207,7 @@ __global__ void k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__
     const int c = q.ent;
     const int n = ld(m.c_n, c);
     M div = mv_fill<R, V>(R(0)), th = mv_fill<R, V>(R(0));
-    for (int k = 0; k < n; k++) {
+    MPSW_SLOTS(k, NB::c, n) {
       const int e = ld(m.c_es, (size_t)k * nC + c);
       const R s = R(m.c_esg[(size_t)k * nC + c]);
       const M ue = ldv<V>(ut + (size_t)e * B + q.b);
@@ -204,13 +221,13 @@ __global__ void k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__
     const R area = ld(m.c_area, c);
     div = div * (R(1) / area);
     M ke = mv_fill<R, V>(R(0));
-    for (int i = 0; i < n; i++) {
+    MPSW_SLOTS(i, NB::c, n) {
       const int e = ld(m.c_eoc, (size_t)i * nC + c);
       ke = ke + ((R(0.25) * ld(m.e_dc, e)) * ld(m.e_dv, e)) * ((R(2) * ld(bs.u, e)) * ldv<V>(ut + (size_t)e * B + q.b));
     }
     ke = ke / area;
     M pc = mv_fill<R, V>(R(0)), vc = mv_fill<R, V>(R(0));
-    for (int k = 0; k < n; k++) {
+    MPSW_SLOTS(k, NB::c, n) {
       const int v = ld(m.c_vs, (size_t)k * nC + c);
       const R kt = ld(m.c_vk, (size_t)k * nC + c);
       pc = pc + (kt * ldv<V>(d.pvv + (size_t)v * B + q.b)) / area;
@@ -228,7 +245,7 @@ __global__ void k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__
 }
 
 // :319-329, :364-393, :425-445, h_edge_tl :117-126, delsq_u_tl :638-652
-template <typename R, int V>
+template <typename R, int V, class NB>
 __global__ void k_tl_edge_diag(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                                const R *__restrict__ ht, Diag<R> d, Phys<R> ph) {
   using M = Mv<R, V>;
@@ -238,7 +255,7 @@ __global__ void k_tl_edge_diag(MeshDev<R> m, int B, Base<R> bs, const R *__restr
     const int e = q.ent;
     const int n = ld(m.e_n, e);
     M vt = mv_fill<R, V>(R(0));
-    for (int j = 0; j < n; j++)
+    MPSW_SLOTS(j, NB::e2, n)
       vt = vt + ld(m.e_w, (size_t)j * nE + e) * ldv<V>(ut + (size_t)ld(m.e_eoe, (size_t)j * nE + e) * B + q.b);
     const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
     const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
@@ -263,7 +280,7 @@ __global__ void k_tl_edge_diag(MeshDev<R> m, int B, Base<R> bs, const R *__restr
 }
 
 // sw_compute_tend_tlm normal-velocity part :564-768 and the RK update
-template <typename R, typename A, int V>
+template <typename R, typename A, int V, class NB>
 __global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                                const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
                                R *tend_u) {
@@ -276,7 +293,7 @@ __global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restr
     const M pet_e = ldv<V>(d.pe + (size_t)e * B + q.b);
     const R pe_e = ld(bs.pe, e);
     M qt = mv_fill<R, V>(R(0));
-    for (int j = 0; j < n; j++) {
+    MPSW_SLOTS(j, NB::e2, n) {
       const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
       const R w = ld(m.e_w, (size_t)j * nE + e);
       const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + q.b));
@@ -316,6 +333,127 @@ __global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restr
     if (tend_u) stv<V>(tend_u + o, tut);
     rk_members<R, A, V>(rk, o, tut);
   }
+}
+
+// ---- edgesOnEdge lists staged in shared memory --------------------------------------------
+// A block of the staged edge kernels handles `epb` consecutive edges with B / V threads each.
+// Before the member work, the block copies the edgesOnEdge lists of its edges (neighbour index,
+// weight and up to three per-edge fields of the linearisation point at the neighbour) into
+// shared memory, slot-major ([J][epb]), with coalesced loads spread over all its threads; the
+// member loads of every slot then take their addresses from shared memory, so each thread's
+// loads no longer wait on an index load from global memory first.
+template <typename R, int J, int NF>
+struct EoeStage {
+  const int *nb;      // [J][epb] neighbour edge (0 past the edge's list)
+  const R *w;         // [J][epb] weight (0 past the list)
+  const R *f[NF];     // [J][epb] field k at the neighbour
+  int epb;
+  __device__ int at(int j, int le) const { return j * epb + le; }
+};
+
+// Shared-memory bytes of an EoeStage for `epb` edges.
+template <typename R, int J, int NF>
+constexpr size_t eoe_stage_bytes(int epb) {
+  return (size_t)J * epb * (sizeof(int) + (1 + NF) * sizeof(R));
+}
+
+// Fill the stage of edges e0 .. e0 + epb - 1 (weights from `wts`: weightsOnEdge or its transpose)
+// and __syncthreads.  Every thread of the block must call it.
+template <typename R, int J, int NF>
+__device__ EoeStage<R, J, NF> stage_eoe(const MeshDev<R> &m, const R *wts, int e0, int epb,
+                                        const R *const (&fields)[NF]) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sw = reinterpret_cast<R *>(smem_raw);
+  R *sf = sw + (size_t)J * epb;
+  int *snb = reinterpret_cast<int *>(sf + (size_t)NF * J * epb);
+  const int nE = m.nE;
+  for (int i = threadIdx.x; i < J * epb; i += blockDim.x) {
+    const int j = i / epb, le = i - j * epb, e = e0 + le;
+    int nb = 0;
+    R w = R(0);
+    R f[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) f[k] = R(0);
+    if (e < nE && j < ld(m.e_n, e)) {
+      nb = ld(m.e_eoe, (size_t)j * nE + e);
+      w = ld(wts, (size_t)j * nE + e);
+#pragma unroll
+      for (int k = 0; k < NF; k++) f[k] = ld(fields[k], nb);
+    }
+    snb[i] = nb;
+    sw[i] = w;
+#pragma unroll
+    for (int k = 0; k < NF; k++) sf[(size_t)k * J * epb + i] = f[k];
+  }
+  __syncthreads();
+  EoeStage<R, J, NF> st;
+  st.nb = snb;
+  st.w = sw;
+#pragma unroll
+  for (int k = 0; k < NF; k++) st.f[k] = sf + (size_t)k * J * epb;
+  st.epb = epb;
+  return st;
+}
+
+// k_tl_edge_tend with staged edgesOnEdge lists: one block per `epb` edges, no grid-stride loop.
+template <typename R, typename A, int V, int J>
+__global__ void k_tl_edge_tend_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                                  const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
+                                  R *tend_u) {
+  using M = Mv<R, V>;
+  pdl_begin();
+  const int tpe = B / V, epb = blockDim.x / tpe;
+  const int e0 = blockIdx.x * epb;
+  const R *const fields[3] = {bs.pe, bs.u, bs.he};
+  const EoeStage<R, J, 3> st = stage_eoe<R, J, 3>(m, m.e_w, e0, epb, fields);
+  const int le = threadIdx.x / tpe;
+  const int e = e0 + le;
+  if (le >= epb || e >= m.nE) return;
+  const int b = (threadIdx.x - le * tpe) * V;
+  const int n = ld(m.e_n, e);
+  const M pet_e = ldv<V>(d.pe + (size_t)e * B + b);
+  const R pe_e = ld(bs.pe, e);
+  M qt = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(j, J, n) {
+    const int i = st.at(j, le);
+    const int eoe = st.nb[i];
+    const R w = st.w[i];
+    const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + b));
+    const R wpv = R(0.5) * (pe_e + st.f[0][i]);
+    const R ub = st.f[1][i], heb = st.f[2][i];
+    qt = qt + ((w * ldv<V>(ut + (size_t)eoe * B + b)) * wpv) * heb + ((w * ub) * wpvt) * heb +
+         ((w * ub) * wpv) * ldv<V>(d.he + (size_t)eoe * B + b);
+  }
+  const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
+  const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
+  M tut = qt - ((ldv<V>(d.ke + (size_t)c2 * B + b) - ldv<V>(d.ke + (size_t)c1 * B + b)) +
+                R(GRAVITY) * (ldv<V>(ht + (size_t)c2 * B + b) - ldv<V>(ht + (size_t)c1 * B + b))) / dc;
+  if (ph.visc2 > R(0)) {
+    M ud = (ldv<V>(d.div + (size_t)c2 * B + b) - ldv<V>(d.div + (size_t)c1 * B + b)) / dc -
+           (ldv<V>(d.vort + (size_t)v2 * B + b) - ldv<V>(d.vort + (size_t)v1 * B + b)) / dv;
+    ud = (ld(m.e_sc2, e) * ph.visc2) * ud;
+    tut = tut + ud;
+  }
+  if (ph.visc4 > R(0)) {
+    M ud = (ldv<V>(d.dsq_div + (size_t)c2 * B + b) - ldv<V>(d.dsq_div + (size_t)c1 * B + b)) / dc -
+           (ldv<V>(d.dsq_vort + (size_t)v2 * B + b) - ldv<V>(d.dsq_vort + (size_t)v1 * B + b)) / dv;
+    ud = (ld(m.e_sc4, e) * ph.visc4) * ud;
+    tut = tut - ud;
+  }
+  const R hh = ld(bs.he, e);
+  const M het = ldv<V>(d.he + (size_t)e * B + b);
+  if (ph.wind) tut = tut - ((het * ld(m.e_usrc, e)) / R(RHO_REF)) / (hh * hh);
+  if (ph.drag) {
+    const M ket_e = R(0.5) * (ldv<V>(d.ke + (size_t)c1 * B + b) + ldv<V>(d.ke + (size_t)c2 * B + b));
+    const R ke_e = R(0.5) * (ld(bs.ke, c1) + ld(bs.ke, c2));
+    const R uu = ld(bs.u, e), sq = sqrt(R(2) * ke_e);
+    tut = tut - ((R(1.0e-3) * ldv<V>(ut + (size_t)e * B + b)) * sq) / hh -
+          ((((R(0.5) * R(1.0e-3)) * uu) * (R(2) * ket_e)) / sq) / hh +
+          (((R(1.0e-3) * uu) * sq) * het) / (hh * hh);
+  }
+  const size_t o = (size_t)e * B + b;
+  if (tend_u) stv<V>(tend_u + o, tut);
+  rk_members<R, A, V>(rk, o, tut);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -361,7 +499,7 @@ __global__ void k_ad_tinit(MeshDev<R> m, int B, const A *x2u, const A *x2h, cons
 // Edge stage: workpv/q adjoint (:689-718) as a gather over the transposed edgesOnEdge,
 // thickness-flux adjoint (:720-736), drag (:549-565), wind (:567-572), then the APVM adjoints
 // of the diagnostics (:193-200, :235-242).
-template <typename R, typename A, int V>
+template <typename R, typename A, int V, class NB>
 __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                           AdWork<R> w) {
   using M = Mv<R, V>;
@@ -373,7 +511,7 @@ __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
     const M Te = ldv<V>(in.tu + (size_t)e * B + q.b);
     const R ue = ld(bs.u, e), hee = ld(bs.he, e), pee = ld(bs.pe, e);
     M pe_ad = mv_fill<R, V>(R(0)), he_ad = mv_fill<R, V>(R(0)), ud = mv_fill<R, V>(R(0));
-    for (int j = 0; j < n; j++) {
+    MPSW_SLOTS(j, NB::e2, n) {
       const int nb = ld(m.e_eoe, (size_t)j * nE + e);
       const R wj = ld(m.e_w, (size_t)j * nE + e);
       const R wr = ld(m.e_wrev, (size_t)j * nE + e);
@@ -417,7 +555,7 @@ __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
 
 // del4 adjoint, first half (:588-634): delsq_vorticity/delsq_circulation adjoint on vertices
 // and delsq_divergence adjoint on cells.
-template <typename R, int V>
+template <typename R, int V, class NB>
 __global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R> in, AdWork<R> w) {
   using M = Mv<R, V>;
   const int nV = m.nV, nC = m.nC;
@@ -440,7 +578,7 @@ __global__ void k_ad_del4_vc(MeshDev<R> m, int B, Phys<R> ph, AdIn<R> in, AdWork
       const int c = q.ent;
       const int n = ld(m.c_n, c);
       M acc = mv_fill<R, V>(R(0));
-      for (int k = 0; k < n; k++) {
+      MPSW_SLOTS(k, NB::c, n) {
         const int e = ld(m.c_es, (size_t)k * nC + c);
         const R sg = R(m.c_esg[(size_t)k * nC + c]);
         const M ud4 = (ld(m.e_sc4, e) * ph.visc4) * (-ldv<V>(in.tu + (size_t)e * B + q.b));
@@ -472,7 +610,7 @@ __global__ void k_ad_del4_e(MeshDev<R> m, int B, AdWork<R> w) {
 // Cell stage: gradPVn adjoint onto pv_cell (:202-213), gravity/ke terms of the tendency
 // adjoint (:696-699), drag ke terms, del2/del4 divergence adjoints, h_edge adjoint (:358-369),
 // then the 1/areaCell scalings of ke_ad and divergence_ad (:306-326).
-template <typename R, typename A, int V>
+template <typename R, typename A, int V, class NB>
 __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                           AdWork<R> w) {
   using M = Mv<R, V>;
@@ -485,7 +623,7 @@ __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
     M ke_ad = mv_fill<R, V>(sd.ke ? sd.ke[c] : R(0));
     M div_ad = mv_fill<R, V>(sd.div ? sd.div[c] : R(0));
     M hd = mv_fill<R, V>(R(0));
-    for (int k = 0; k < n; k++) {
+    MPSW_SLOTS(k, NB::c, n) {
       const int e = ld(m.c_es, (size_t)k * nC + c);
       const R sg = R(m.c_esg[(size_t)k * nC + c]);
       const size_t oe = (size_t)e * B + q.b;
@@ -608,7 +746,7 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
 // Final stage of the adjoint: h_vertex -> h (:286-289) on cells, and on edges the transposed
 // tangential velocity (:296-303), ke (:306-317), divergence (:327-340) and circulation
 // (:350-355) adjoints.  Cell threads then edge threads.
-template <typename R, typename A, int V>
+template <typename R, typename A, int V, class NB>
 __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out) {
   using M = Mv<R, V>;
   const int nC = m.nC, nE = m.nE;
@@ -619,7 +757,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
       const int c = q.ent;
       const int n = ld(m.c_n, c);
       M ph_ = ldv<V>(w.hd + (size_t)c * B + q.b);
-      for (int k = 0; k < n; k++)
+      MPSW_SLOTS(k, NB::c, n)
         ph_ = ph_ + ld(m.c_vk, (size_t)k * nC + c) * ldv<V>(w.hv_ad + (size_t)ld(m.c_vs, (size_t)k * nC + c) * B + q.b);
       ad_emit<R, A, V>(out, 0, (size_t)c * B + q.b, ph_, ld(m.c_area, c));
     } else {
@@ -627,7 +765,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
       const int e = q.ent;
       const int n = ld(m.e_n, e);
       M pu = ldv<V>(w.ud + (size_t)e * B + q.b);
-      for (int j = 0; j < n; j++) {
+      MPSW_SLOTS(j, NB::e2, n) {
         const int nb = ld(m.e_eoe, (size_t)j * nE + e);
         pu = pu + ld(m.e_wrev, (size_t)j * nE + e) * ldv<V>(w.v_ad + (size_t)nb * B + q.b);
       }

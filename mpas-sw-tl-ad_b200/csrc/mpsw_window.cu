@@ -690,6 +690,18 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
       case 1: LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream); break;
       case 2: LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream); break;
       case 3: LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream); break;
+      case 8:  // one whole tangent-linear stage
+        LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], mb->d, E.stream);
+        LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream);
+        LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream);
+        if (ph.visc4 > R(0)) LR::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
+        LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream);
+        break;
+      case 9: {  // one whole adjoint stage
+        const AdSeeds<R> none{};
+        LR::ad_stage(m, B, bs, ph, in, none, mb->w, out, E.stream);
+        break;
+      }
       default: LR::ad_part(which - 4, m, B, bs, ph, in, mb->w, out, E.stream); break;
     }
   };
@@ -711,7 +723,7 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
 
 double Engine::time_kernel(int which, int prec, int B, int iters) {
   if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
-  if (which < 0 || which > 7 || B < 1 || iters < 1) throw EngineError(MPSW_ERR_ARG, "bad kernel timing request");
+  if (which < 0 || which > 9 || B < 1 || iters < 1) throw EngineError(MPSW_ERR_ARG, "bad kernel timing request");
   return prec == 1 ? time_kernel_impl<float>(*this, which, prec, B, iters)
                    : time_kernel_impl<double>(*this, which, prec, B, iters);
 }
