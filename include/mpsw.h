@@ -98,6 +98,9 @@ int mpsw_state_to_device(mpsw_handle *h, double *u, double *hh, void *stream);
  * and, as the storage mode selects, as the linearisation point of every RK stage of every
  * step; tangent-linear and adjoint sweeps read stored stages, or recompute states and stages
  * from the checkpoints where that precision is not stored (identical results either way).
+ * The call copies the start state; the forward sweep itself runs in the first window call
+ * that follows, alongside the members when that call is a tangent-linear sweep over a stored
+ * precision, with the physics settings in force then.
  * precision: 0 = FP64 throughout, 1 = FP32 stencils with FP64 RK accumulation. */
 int mpsw_window_init(mpsw_handle *h, int nsteps, int ckpt_every, void *stream);
 /* Storage mode of the following mpsw_window_init calls.  No counterpart in the reference

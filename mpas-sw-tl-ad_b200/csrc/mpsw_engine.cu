@@ -191,6 +191,9 @@ Engine::Engine() {
 void Engine::need_device() {
   if (stream) return;
   cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (cudaEvent_t *ev : {&ev_fork, &ev_step, &ev_join})
+    cuda_check(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 Engine::~Engine() {
@@ -200,6 +203,9 @@ Engine::~Engine() {
   free_device_mesh();
   for (void *p : work) cudaFree(p);
   window_free();
+  for (cudaEvent_t ev : {ev_fork, ev_step, ev_join})
+    if (ev) cudaEventDestroy(ev);
+  if (side) cudaStreamDestroy(side);
   if (stream) cudaStreamDestroy(stream);
 }
 

@@ -39,6 +39,7 @@ struct Var {
 // Storage of the batched tangent-linear / adjoint window (mpsw_window_*).
 struct Window {
   int nsteps = 0, every = 0, nckpt = 0;
+  bool pending = false;  // start state captured in x_u / x_h, forward sweep not yet run
   std::vector<double *> ck_u, ck_h;    // checkpointed nonlinear states (internal order)
   double *seg_u = nullptr, *seg_h = nullptr;  // states of one segment, [every][n]
   double *fin_u = nullptr, *fin_h = nullptr;  // final state
@@ -66,6 +67,9 @@ struct Window {
     std::vector<void *> mem;
     void *bufs = nullptr;  // MemberBufs<R>
     double *acc_u = nullptr, *acc_h = nullptr;
+    // the members' FP64 states during a sweep: callers' buffers are copied in and out, so the
+    // captured graphs do not depend on where the caller keeps its members
+    double *x_u = nullptr, *x_h = nullptr;
   } ms[2];
 };
 
@@ -98,6 +102,8 @@ struct Engine {
   bool allocated[3] = {false, false, false};
   int nC = 0, nE = 0, nV = 0, mE = 0, mE2 = 0, vd = 0, nT = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;                 // second stream for work forked inside a graph
+  cudaEvent_t ev_fork = nullptr, ev_step = nullptr, ev_join = nullptr;
 
   // device mesh
   bool mesh_built = false, mesh_dirty = true;
@@ -188,7 +194,9 @@ struct Engine {
   void window_storage(int mode, double max_bytes);
   void window_store_alloc(int nsteps);
   void window_store_free(int prec);
-  void window_trajectory(cudaStream_t s);
+  void window_capture_state(cudaStream_t s);
+  void window_forward();
+  void window_ensure();
   void window_tl(int prec, int B, double *du, double *dh, cudaStream_t s);
   void window_ad(int prec, int B, double *au, double *ah, cudaStream_t s);
   void window_final(double *u, double *h, cudaStream_t s);

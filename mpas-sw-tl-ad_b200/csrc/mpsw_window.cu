@@ -50,6 +50,7 @@ void free_members(Window::Members &M) {
   M.bufs = nullptr;
   M.B = 0;
   M.acc_u = M.acc_h = nullptr;
+  M.x_u = M.x_h = nullptr;
 }
 
 template <typename R>
@@ -84,6 +85,8 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   }
   M.acc_u = walloc<double>(M, Ed, s);
   M.acc_h = walloc<double>(M, C, s);
+  M.x_u = walloc<double>(M, Ed, s);
+  M.x_h = walloc<double>(M, C, s);
   M.bufs = mb;
   M.B = B;
   return mb;
@@ -167,6 +170,8 @@ GraphKey Engine::graph_key(int kind, int prec, int B, const void *p1, const void
 // Run `body` (kernel launches on the engine stream, no allocation, no synchronisation) as a
 // CUDA graph: captured on first use for this key, replayed afterwards.  MPSW_GRAPHS=0 runs it
 // eagerly instead.
+constexpr size_t kMaxGraphs = 24;
+
 template <typename F>
 void Engine::run_graph(const GraphKey &k, F &&body) {
   static const bool enabled = !(getenv("MPSW_GRAPHS") && atoi(getenv("MPSW_GRAPHS")) == 0);
@@ -174,12 +179,18 @@ void Engine::run_graph(const GraphKey &k, F &&body) {
     body();
     return;
   }
-  for (auto &g : graphs)
-    if (g.key == k) {
+  for (size_t i = 0; i < graphs.size(); i++)
+    if (graphs[i].key == k) {
+      if (i + 1 < graphs.size()) std::rotate(graphs.begin() + i, graphs.begin() + i + 1, graphs.end());
+      GraphEntry &g = graphs.back();  // most recently used last
       cuda_check(cudaGraphLaunch(g.exec, stream), "cudaGraphLaunch");
       g_launches += g.kernels;
       return;
     }
+  if (graphs.size() >= kMaxGraphs) {  // evict the least recently used
+    cudaGraphExecDestroy(graphs.front().exec);
+    graphs.erase(graphs.begin());
+  }
   cudaGraph_t graph = nullptr;
   const long long before = g_launches;
   cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -353,7 +364,7 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
   if (W.nsteps && W.every == ev && W.nckpt == nck && W.x_u) {
     W.nsteps = nsteps;  // same checkpoint layout: reuse every buffer
     window_store_alloc(nsteps);
-    window_trajectory(s);
+    window_capture_state(s);
     return;
   }
   window_free_trajectory();
@@ -394,51 +405,73 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
     W.sh[k] = k == 0 ? nullptr : D(nC);
   }
   window_store_alloc(nsteps);
-  window_trajectory(s);
+  window_capture_state(s);
 }
 
-// Forward over the window from the module's level-1 state, checkpointing every `every` steps
-// and, when stores are allocated, writing every stage's linearisation point to them (the
-// whole window is then one CUDA graph, since every step writes different slots).
-void Engine::window_trajectory(cudaStream_t s) {
+// The window starts from the module's level-1 state as it is now: copy it (after the caller's
+// stream) and leave the forward sweep to the first call that needs it (window_ensure), which
+// lets a tangent-linear sweep over stored stages run it alongside.
+void Engine::window_capture_state(cudaStream_t s) {
   Window &W = win;
-  const int nsteps = W.nsteps;
-  const bool storing = W.st[0].mem || W.st[1].mem;
   cuda_check(cudaStreamSynchronize(s), "window sync");
   cuda_check(cudaMemcpyAsync(W.x_u, dv("u"), sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "copy");
   cuda_check(cudaMemcpyAsync(W.x_h, dv("h"), sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "copy");
-  auto ckpt = [&](int n) {
-    if (n % W.every == 0) {
-      cuda_check(cudaMemcpyAsync(W.ck_u[n / W.every], W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "ckpt");
-      cuda_check(cudaMemcpyAsync(W.ck_h[n / W.every], W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "ckpt");
-    }
-  };
-  if (storing) {
+  cuda_check(cudaStreamSynchronize(stream), "window_init");
+  for (int p = 0; p < 2; p++) W.st[p].valid = 0;
+  W.pending = true;
+}
+
+static void window_checkpoint(Engine &E, int n) {
+  Window &W = E.win;
+  if (n % W.every == 0) {
+    cuda_check(cudaMemcpyAsync(W.ck_u[n / W.every], W.x_u, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "ckpt");
+    cuda_check(cudaMemcpyAsync(W.ck_h[n / W.every], W.x_h, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "ckpt");
+  }
+}
+
+// After the forward sweep: keep the final state, mark the stores written.
+static void window_forward_done(Engine &E) {
+  Window &W = E.win;
+  cuda_check(cudaMemcpyAsync(W.fin_u, W.x_u, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "final");
+  cuda_check(cudaMemcpyAsync(W.fin_h, W.x_h, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "final");
+  cuda_check(cudaGetLastError(), "window forward");
+  for (int p = 0; p < 2; p++) W.st[p].valid = W.st[p].mem ? W.nsteps : 0;
+  W.pending = false;
+}
+
+// Forward over the window from the captured start state, checkpointing every `every` steps
+// and, when stores are allocated, writing every stage's linearisation point to them (the
+// whole window is then one CUDA graph, since every step writes different slots).
+void Engine::window_forward() {
+  Window &W = win;
+  const int nsteps = W.nsteps;
+  if (W.st[0].mem || W.st[1].mem) {
     GraphKey key = graph_key(6, 0, nsteps, W.st[0].mem, W.st[1].mem);
     key.n2 = W.every;
     run_graph(key, [&]() {
       for (int n = 0; n < nsteps; n++) {
-        ckpt(n);
+        window_checkpoint(*this, n);
         traj_step(*this, true, 0, [](int) {}, n);
       }
     });
   } else {
     for (int n = 0; n < nsteps; n++) {
-      ckpt(n);
+      window_checkpoint(*this, n);
       run_graph(graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(*this, true, 0, [](int) {}); });
     }
   }
-  cuda_check(cudaMemcpyAsync(W.fin_u, W.x_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "final");
-  cuda_check(cudaMemcpyAsync(W.fin_h, W.x_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "final");
-  cuda_check(cudaGetLastError(), "window_init");
-  cuda_check(cudaStreamSynchronize(stream), "window_init");
-  for (int p = 0; p < 2; p++) W.st[p].valid = W.st[p].mem ? nsteps : 0;
+  window_forward_done(*this);
+}
+
+void Engine::window_ensure() {
+  if (win.pending) window_forward();
 }
 
 // Member work of tangent-linear stage k about the linearisation point bs.
 template <typename R>
 static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, MemberBufs<R> *mb,
-                            const Phys<R> &ph, const double w[4], const double c[4], int k, const Base<R> &bs) {
+                            const Phys<R> &ph, const double w[4], const double c[4], int k, const Base<R> &bs,
+                            cudaStream_t st) {
   Window &W = E.win;
   const MeshDev<R> &m = mesh_for<R>(E);
   const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
@@ -449,8 +482,8 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
       uti = du;
       hti = dh;
     } else {
-      convert_d2f((long long)E.nE * B, du, mb->pu[2], E.stream);
-      convert_d2f((long long)E.nC * B, dh, mb->ph[2], E.stream);
+      convert_d2f((long long)E.nE * B, du, mb->pu[2], st);
+      convert_d2f((long long)E.nC * B, dh, mb->ph[2], st);
       uti = mb->pu[2];
       hti = mb->ph[2];
     }
@@ -459,22 +492,52 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
   RK<R, double> rut{du, k == 0 ? du : acu, k == 3 ? du : acu, k < 3 ? mb->pu[k] : nullptr, c[k], w[k], R(0), ph.tc1};
   RK<R, double> rht{dh, k == 0 ? dh : ach, k == 3 ? dh : ach, k < 3 ? mb->ph[k] : nullptr, c[k], w[k], R(0), 0};
   // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
-  Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, E.stream);
-  Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, E.stream);
-  Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, E.stream);
-  if (ph.visc4 > R(0)) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
-  Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, E.stream);
+  Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, st);
+  Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, st);
+  Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, st);
+  if (ph.visc4 > R(0)) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, st);
+  Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, st);
+}
+
+// Copy B members' FP64 states between a caller's buffers and the engine's (internal order).
+static void members_copy(Engine &E, int B, double *dst_u, double *dst_h, const double *src_u, const double *src_h) {
+  cuda_check(cudaMemcpyAsync(dst_u, src_u, sizeof(double) * E.nE * B, cudaMemcpyDeviceToDevice, E.stream), "members");
+  cuda_check(cudaMemcpyAsync(dst_h, src_h, sizeof(double) * E.nC * B, cudaMemcpyDeviceToDevice, E.stream), "members");
 }
 
 template <typename R>
-static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
+static void window_tl_impl(Engine &E, int prec, int B, double *user_u, double *user_h) {
   Window &W = E.win;
   MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
+  double *du = W.ms[prec].x_u, *dh = W.ms[prec].x_h;
+  members_copy(E, B, du, dh, user_u, user_h);
   const Phys<double> ph64 = E.phys();
   const Phys<R> ph = phys_as<R>(ph64);
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
-  if (W.st[prec].valid >= W.nsteps) {
+  if (W.pending && W.st[prec].mem) {
+    // forward sweep and tangent linear in one graph: the forward on the engine stream, the
+    // members on the side stream, step n of the members after step n of the forward has
+    // stored its stages, so the thin forward kernels run alongside the member kernels
+    GraphKey key = E.graph_key(7, prec, B, du, dh);
+    key.p3 = W.st[prec].mem;
+    key.n2 = ((long long)W.nsteps << 20) | W.every;
+    E.run_graph(key, [&]() {
+      cuda_check(cudaEventRecord(E.ev_fork, E.stream), "event record");
+      cuda_check(cudaStreamWaitEvent(E.side, E.ev_fork, 0), "event wait");
+      for (int n = 0; n < W.nsteps; n++) {
+        window_checkpoint(E, n);
+        traj_step(E, true, 0, [](int) {}, n);
+        cuda_check(cudaEventRecord(E.ev_step, E.stream), "event record");
+        cuda_check(cudaStreamWaitEvent(E.side, E.ev_step, 0), "event wait");
+        for (int k = 0; k < 4; k++)
+          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k), E.side);
+      }
+      cuda_check(cudaEventRecord(E.ev_join, E.side), "event record");
+      cuda_check(cudaStreamWaitEvent(E.stream, E.ev_join, 0), "event wait");
+    });
+    window_forward_done(E);
+  } else if (W.st[prec].valid >= W.nsteps) {
     // stored linearisation points: the whole sweep is one graph of member kernels
     GraphKey key = E.graph_key(4, prec, B, du, dh);
     key.p3 = W.st[prec].mem;
@@ -482,9 +545,10 @@ static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
     E.run_graph(key, [&]() {
       for (int n = 0; n < W.nsteps; n++)
         for (int k = 0; k < 4; k++)
-          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k));
+          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k), E.stream);
     });
   } else {
+    E.window_ensure();
     cuda_check(cudaMemcpyAsync(W.x_u, W.ck_u[0], sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
     cuda_check(cudaMemcpyAsync(W.x_h, W.ck_h[0], sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
     // recompute each step's stages; the member work of stage k runs right after stage k (the
@@ -492,9 +556,10 @@ static void window_tl_impl(Engine &E, int prec, int B, double *du, double *dh) {
     const GraphKey key = E.graph_key(2, prec, B, du, dh);
     for (int n = 0; n < W.nsteps; n++)
       E.run_graph(key, [&]() {
-        traj_step(E, true, prec, [&](int k) { tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, base_for<R>(W, k)); });
+        traj_step(E, true, prec, [&](int k) { tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, base_for<R>(W, k), E.stream); });
       });
   }
+  members_copy(E, B, user_u, user_h, du, dh);
   cuda_check(cudaGetLastError(), "window_tl");
 }
 
@@ -528,9 +593,11 @@ static void ad_member_step(Engine &E, int prec, int B, double *au, double *ah, M
 }
 
 template <typename R>
-static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
+static void window_ad_impl(Engine &E, int prec, int B, double *user_u, double *user_h) {
   Window &W = E.win;
   MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
+  double *au = W.ms[prec].x_u, *ah = W.ms[prec].x_h;
+  members_copy(E, B, au, ah, user_u, user_h);
   const MeshDev<R> &m = mesh_for<R>(E);
   const Phys<double> ph64 = E.phys();
   const Phys<R> ph = phys_as<R>(ph64);
@@ -552,6 +619,7 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
       for (int n = W.nsteps - 1; n >= 0; n--)
         ad_member_step<R>(E, prec, B, au, ah, mb, ph, w, c, [&](int k) { return stored_base<R>(W, prec, n, k); });
     });
+    members_copy(E, B, user_u, user_h, au, ah);
     cuda_check(cudaGetLastError(), "window_ad");
     return;
   }
@@ -576,6 +644,7 @@ static void window_ad_impl(Engine &E, int prec, int B, double *au, double *ah) {
       });
     }
   }
+  members_copy(E, B, user_u, user_h, au, ah);
   cuda_check(cudaGetLastError(), "window_ad");
 }
 
@@ -609,6 +678,7 @@ void Engine::window_ad(int prec, int B, double *au, double *ah, cudaStream_t s) 
   if (B < 1 || !au || !ah) throw EngineError(MPSW_ERR_ARG, "window_ad needs B >= 1 and member buffers");
   if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
   join(s, stream, true);
+  window_ensure();
   if (prec == 0) window_ad_impl<double>(*this, prec, B, au, ah);
   else if (prec == 1) window_ad_impl<float>(*this, prec, B, au, ah);
   else throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
@@ -618,6 +688,7 @@ void Engine::window_ad(int prec, int B, double *au, double *ah, cudaStream_t s) 
 void Engine::window_final(double *u, double *h, cudaStream_t s) {
   if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
   join(s, stream, true);
+  window_ensure();
   cuda_check(cudaMemcpyAsync(u, win.fin_u, sizeof(double) * nE, cudaMemcpyDeviceToDevice, stream), "final u");
   cuda_check(cudaMemcpyAsync(h, win.fin_h, sizeof(double) * nC, cudaMemcpyDeviceToDevice, stream), "final h");
   join(s, stream, false);
@@ -724,6 +795,7 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
 double Engine::time_kernel(int which, int prec, int B, int iters) {
   if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
   if (which < 0 || which > 9 || B < 1 || iters < 1) throw EngineError(MPSW_ERR_ARG, "bad kernel timing request");
+  window_ensure();
   return prec == 1 ? time_kernel_impl<float>(*this, which, prec, B, iters)
                    : time_kernel_impl<double>(*this, which, prec, B, iters);
 }
