@@ -37,10 +37,13 @@ def parse():
     p.add_argument('--steps', type=int, default=3)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='mpsw', choices=['mpsw', 'reference'])
+    p.add_argument('--workload', default='tlad', choices=['tlad', 'fwd'],
+                   help='tlad: batched TL+AD gradients (level 5, 288 steps of 300 s, B=64); '
+                        'fwd: nonlinear forward with mountains (level 7, 1152 steps of 75 s), sim-days/s')
     p.add_argument('--batch', type=int, default=64)
-    p.add_argument('--level', type=int, default=5)
-    p.add_argument('--nsteps', type=int, default=288)
-    p.add_argument('--dt', type=float, default=300.0)
+    p.add_argument('--level', type=int, default=None)
+    p.add_argument('--nsteps', type=int, default=None)
+    p.add_argument('--dt', type=float, default=None)
     p.add_argument('--ckpt', type=int, default=16)
     p.add_argument('--storage', type=int, default=-1,
                    help='stage storage mode of the window: -1 auto, 0 checkpoints only, 1 FP64, 2 FP32, 3 both')
@@ -50,7 +53,12 @@ def parse():
                         'the NVTX range "mpsw_kernels", as mpsw_time_kernel launches them; no JSON line')
     p.add_argument('--profile', action='store_true',
                    help='only the timed batched windows (for profiler launch lists); no JSON line')
-    return p.parse_args()
+    a = p.parse_args()
+    dflt = {'tlad': (5, 288, 300.0), 'fwd': (7, 1152, 75.0)}[a.workload]
+    a.level = dflt[0] if a.level is None else a.level
+    a.nsteps = dflt[1] if a.nsteps is None else a.nsteps
+    a.dt = dflt[2] if a.dt is None else a.dt
+    return a
 
 
 def workload(level, dt):
@@ -463,6 +471,169 @@ def run_mpsw(a, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def forward_bytes(nC, nE, nV, sum_eoe, s, a=8):
+    """Algorithmic bytes of one RK4 step of one trajectory: per stage the mesh once,
+    M(s) = 4 (2E + 2E + S + E + 2E + N + 3V + 3V) + s (S + 2E + 2N + 3V + 2V), and the state
+    S = (N + E)(2s + 3a) (read x_k, write x_k+1 at s; x0 and the accumulator at a)."""
+    E, N, V, S = nE, nC, nV, sum_eoe
+    mesh = 4 * (2 * E + 2 * E + S + E + 2 * E + N + 3 * V + 3 * V) + s * (S + 2 * E + 2 * N + 3 * V + 2 * V)
+    return 4 * (mesh + (N + E) * (2 * s + 3 * a))
+
+
+def _oracle_forward_sample(args):
+    """Seconds per sw_rk4 step of the oracle on the forward workload (host, one core)."""
+    level, dt, n = args
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    m = O.OracleModule()
+    forward_module(m, level, dt)
+    m.sw_mpas_init_block()
+    m.sw_rk4()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        m.sw_rk4()
+    return (time.perf_counter() - t0) / n
+
+
+def forward_module(mod, level, dt):
+    """Seeded balanced flow over seeded mountains (h reduced by the topography)."""
+    from mpsw import ic
+    unit, mesh, st = workload(level, dt)
+    load_module(mod, unit, mesh, st, dt)
+    b = ic.mountains(mesh, 1000)
+    mod.h_s = b[None, :]
+    mod.h[0, 0] = st['h'] - b
+    return unit
+
+
+def run_forward(a, rank, world):
+    """Nonlinear forward over one day: FP32 stencils + FP64 accumulation (the value) beside the
+    plain FP64 form, each timed on the engine's stream; errors against the FP64 GPU run."""
+    import ctypes
+    import numpy as np
+    import torch
+    from module_sw_mpas import MpasSwModule
+    from mpsw import _lib, replicas
+
+    dev = rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    mod = MpasSwModule()
+    unit = forward_module(mod, a.level, a.dt)
+    mod.sw_mpas_init_block()
+    L = _lib.load()
+    h = mod.handle
+    sp = ctypes.c_void_p()
+    h.check(L.mpsw_get_stream(h.ptr, ctypes.byref(sp)), 'get_stream')
+    stream = torch.cuda.ExternalStream(sp.value)
+    nC, nE, nV = unit['nCells'], unit['nEdges'], unit['nVertices']
+    u0 = torch.tensor(np.ascontiguousarray(mod.u[0, 0]), device='cuda')
+    h0 = torch.tensor(np.ascontiguousarray(mod.h[0, 0]), device='cuda')
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+
+    def reset():
+        torch.cuda.synchronize()
+        h.check(L.mpsw_state_from_device(h.ptr, ctypes.c_void_p(u0.data_ptr()), ctypes.c_void_p(h0.data_ptr()),
+                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), 'state')
+
+    def run(prec, n_warm, n_time):
+        times = []
+        launches0 = L.mpsw_launch_count()
+        for i in range(n_warm + n_time):
+            reset()
+            flush.zero_()
+            torch.cuda.synchronize()
+            replicas_barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.check(L.mpsw_forward(h.ptr, prec, a.nsteps), 'forward')
+            e1.record(stream)
+            torch.cuda.synchronize()
+            replicas_barrier()
+            if i >= n_warm:
+                times.append(e0.elapsed_time(e1))
+            else:
+                launches0 = L.mpsw_launch_count()
+        return sum(times) / len(times), (L.mpsw_launch_count() - launches0) / max(1, n_time)
+
+    def replicas_barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def state():
+        out_u = torch.empty(nE, dtype=torch.float64, device='cuda')
+        out_h = torch.empty(nC, dtype=torch.float64, device='cuda')
+        h.check(L.mpsw_state_to_device(h.ptr, ctypes.c_void_p(out_u.data_ptr()), ctypes.c_void_p(out_h.data_ptr()),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), 'state')
+        torch.cuda.synchronize()
+        return out_u, out_h
+
+    days = a.nsteps * a.dt / 86400.0
+    with Clocks(dev) as clk:
+        ms32, launches = run(1, a.warmup, a.steps)
+    clocks = clk.summary()
+    ms32 = replicas.max_over_ranks(ms32, device='cuda')
+    u32, h32 = state()
+    ms64, _ = run(0, 1, max(1, min(a.steps, 2)))
+    ms64 = replicas.max_over_ranks(ms64, device='cuda')
+    u64, h64 = state()
+    err = {'u': float(torch.linalg.norm(u32 - u64) / torch.linalg.norm(u64)),
+           'h': float(torch.linalg.norm(h32 - h64) / torch.linalg.norm(h64))}
+    value = world * days / (ms32 / 1e3)
+
+    # end to end through the module surface: host state in, host state out, every run
+    hu, hh = u0.cpu().numpy(), h0.cpu().numpy()
+    te = []
+    for i in range(1 + a.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mod.u[0, 0] = hu
+        mod.h[0, 0] = hh
+        mod.sw_rk4_steps(a.nsteps, 1)
+        out = mod.h[0, 0].copy(), mod.u[0, 0].copy()
+        if i:
+            te.append(time.perf_counter() - t0)
+    e2e = world * days / (sum(te) / len(te))
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json')))
+    except Exception:
+        pass
+    hbm = peaks.get('hbm_gbs') or 6650.0
+    sum_eoe = int(unit['nEdgesOnEdge'].sum())
+    bytes_step = forward_bytes(nC, nE, nV, sum_eoe, 4)
+    ach = bytes_step / (ms32 / 1e3 / a.nsteps) / 1e9
+    cpu = None
+    if rank == 0:
+        sample = 3
+        per = _oracle_forward_sample((a.level, a.dt, sample))
+        cpu = {'value': days / (per * a.nsteps), 'unit': 'sim-days/s', 'cores': 1, 'kind': 'port',
+               'sample': '%d sw_rk4 steps of the oracle, extrapolated to %d steps' % (sample, a.nsteps)}
+    if rank == 0:
+        line = {
+            'metric': 'sim-days/s, nonlinear forward, FP32 stencils + FP64 accumulation (error vs FP64 GPU)',
+            'value': value, 'unit': 'sim-days/s', 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
+            'ms_per_step': ms32, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32 stencils + f64 accumulation',
+            'data': 'synthetic (seeded balanced flow over 8 seeded mountains, level-%d TRiSK mesh)' % a.level,
+            'config': {'workload': 'forward: level-%d mesh (%d cells), %d RK4 steps of %g s (%.2f days)' % (a.level, nC, a.nsteps, a.dt, days),
+                       'parallelism': 'replicas x%d' % world,
+                       'l2': 'flushed (256 MB write) between timed runs; state + mesh ~%.0f MB' % ((nC + nE) * 8 * 10 / 1e6 + 300 * nC / 1e6)},
+            'fp64_sim_days_per_s': world * days / (ms64 / 1e3),
+            'rel_err_fp32_vs_fp64': err,
+            'e2e': {'value': e2e, 'unit': 'sim-days/s', 'h2d_bytes_per_step': int((nC + nE) * 8),
+                    'd2h_bytes_per_step': int((nC + nE) * 8)},
+            'roofline': {'bound': 'hbm', 'kernel': 'one RK4 step (20 launches)', 'achieved': ach, 'peak': hbm,
+                         'unit': 'GB/s', 'frac': ach / hbm, 'traffic': None, 'algorithmic_bytes': bytes_step,
+                         'peak_source': 'measured' if peaks.get('hbm_gbs') else 'fallback'},
+            'cpu_baseline': cpu,
+            'clocks': clocks,
+            'gpu_launches': int(launches),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get('RANK', '0'))
@@ -476,6 +647,8 @@ def main():
             dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
     if a.impl == 'reference':
         run_reference(a, rank, world)
+    elif a.workload == 'fwd':
+        run_forward(a, rank, world)
     else:
         run_mpsw(a, rank, world)
     if world > 1 and a.impl == 'mpsw':

@@ -67,6 +67,11 @@ int mpsw_sw_mpas_init_block(mpsw_handle *h);  /* :495-526 */
 int mpsw_sw_rk4(mpsw_handle *h, int nsteps);      /* :528-635, nsteps consecutive calls */
 int mpsw_sw_rk4_tlm(mpsw_handle *h, int nsteps);  /* :637-781 */
 int mpsw_sw_rk4_adj(mpsw_handle *h);              /* :783-1002 */
+/* nsteps RK4 steps of the level-1 state, as nsteps calls of sw_rk4 (:528-635).  precision 0:
+ * identical to mpsw_sw_rk4.  precision 1 (no counterpart in the reference): stencils in FP32
+ * on h - h_ref (h_ref = the mean of h(1) at the call, rounded to a metre) and u, RK4 state and
+ * accumulation in FP64; the module's diagnostics afterwards are the FP64 ones of the new state. */
+int mpsw_forward(mpsw_handle *h, int precision, int nsteps);
 
 /* ---- stencil routines on the level-1 state (module diagnostics in and out) ----------- */
 int mpsw_solve_diagnostics(mpsw_handle *h);      /* sw_compute_solve_diagnostics, dyncore.f90:1-361 */
@@ -138,6 +143,9 @@ int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const double *hh,
                               double *tend_h, void *stream);
 
 /* ---- measurement ----------------------------------------------------------------------- */
+/* The stream the handle's module subroutines run on (a cudaStream_t), so a caller can time
+ * them with events on it. */
+int mpsw_get_stream(mpsw_handle *h, void **stream);
 /* Number of kernels the library has launched in this process (all handles). */
 long long mpsw_launch_count(void);
 /* Average time of `iters` back-to-back launches of one member stencil kernel on the buffers

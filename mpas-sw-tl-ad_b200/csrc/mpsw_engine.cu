@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cctype>
 #include <cstring>
 #include <map>
@@ -253,7 +254,10 @@ void Engine::allocate_group(int g) {
     if (v.ent) {
       const long long ne = v.ent == 1 ? nC : v.ent == 2 ? nE : nV;
       v.lead = (int)(n / ne);
-      if (v.dev) cudaFree(v.dev);
+      if (v.dev) {
+        graphs_free();  // captured launches hold variable pointers
+        cudaFree(v.dev);
+      }
       v.dev = nullptr;      // allocated when a routine first needs the device
       v.dev_valid = false;
     }
@@ -385,6 +389,7 @@ void Engine::fill_mesh(MeshDev<R> &m) {
 }
 
 void Engine::free_device_mesh() {
+  graphs_free();  // captured launches hold mesh pointers
   for (void *p : mesh_bufs) cudaFree(p);
   mesh_bufs.clear();
   mesh_built = false;
@@ -481,6 +486,7 @@ Diag<double> Engine::new_diag(int B) {
 }
 
 void Engine::alloc_work() {
+  graphs_free();  // captured launches hold work-buffer pointers
   for (void *p : work) cudaFree(p);
   work.clear();
   for (int k = 0; k < 5; k++) stage[k] = new_diag(1);
@@ -495,6 +501,16 @@ void Engine::alloc_work() {
   adw.pc_ad = wbuf(nC); adw.ke_ad = wbuf(nC); adw.div_ad = wbuf(nC); adw.hd = wbuf(nC); adw.dd_ad = wbuf(nC);
   adw.hv_ad = wbuf(nV); adw.circ_ad = wbuf(nV); adw.dc_ad = wbuf(nV);
   for (int k = 0; k < 2; k++) { tu_[k] = wbuf(nE); th_[k] = wbuf(nC); }
+  auto fbuf = [&](size_t n) {
+    void *p = dalloc(sizeof(float) * n);
+    work.push_back(p);
+    return (float *)p;
+  };
+  d32 = Diag<float>{};
+  d32.vort = fbuf(nV); d32.hv = fbuf(nV); d32.pvv = fbuf(nV); d32.div = fbuf(nC); d32.ke = fbuf(nC);
+  d32.pc = fbuf(nC); d32.v = fbuf(nE); d32.gpt = fbuf(nE); d32.pe = fbuf(nE); d32.gpn = fbuf(nE);
+  d32.he = fbuf(nE); d32.dsq_u = fbuf(nE); d32.dsq_vort = fbuf(nV); d32.dsq_div = fbuf(nC);
+  for (int k = 0; k < 4; k++) { s32_u[k] = fbuf(nE); s32_h[k] = fbuf(nC); }
   xacc_u = wbuf(nE); xacc_h = wbuf(nC);
 }
 
@@ -651,7 +667,7 @@ void Engine::rk4(int nsteps) {  // src/mpas_sw_module.f90:528-635
   double w[4], c[4];
   rk_coeffs(ph.dt, w, c);
   double *u0 = dv("u"), *h0 = dv("h");
-  for (int step = 0; step < nsteps; step++) {
+  auto step = [&]() {
     for (int k = 0; k < 4; k++) {
       const double *ui = k == 0 ? u0 : sp_u[k - 1];
       const double *hi = k == 0 ? h0 : sp_h[k - 1];
@@ -659,12 +675,73 @@ void Engine::rk4(int nsteps) {  // src/mpas_sw_module.f90:528-635
       RK<double, double> rh{h0, k == 0 ? h0 : acc_h, k == 3 ? h0 : acc_h, k < 3 ? sp_h[k] : nullptr, c[k], w[k], 0.0, 0};
       fwd_stage(ui, hi, stage[0], ph, ru, rh, k == 3 ? dv("tend_u") : nullptr, k == 3 ? dv("tend_h") : nullptr);
     }
-  }
+  };
+  // one CUDA graph per step (its buffers are fixed), captured on the first step
+  const GraphKey key = graph_key(8, 0, 1, u0, h0);
+  for (int n = 0; n < nsteps; n++) run_graph(key, step);
   finish_levels({"u", "h"});
   L64::recon(m64, 1, ph.sphere, u0, dv("uReconstructX"), dv("uReconstructY"), dv("uReconstructZ"),
              dv("uReconstructZonal"), dv("uReconstructMeridional"), stream);
   check_launch("sw_rk4");
   for (const char *n : {"u", "h", "tend_u", "tend_h"}) mark_written(var(n), true);
+  mark_recon(0);
+  mark_diag(0, true);
+  pending_diag = 1;
+}
+
+// nsteps RK4 steps of the level-1 state.  Precision 0 is sw_rk4 repeated (bit-identical);
+// precision 1 runs the stencils in FP32 and keeps the RK4 state and its accumulation in FP64:
+// each step rounds u(1) and h(1) - h_ref to FP32 (h_ref: the mean depth at the call, so FP32
+// carries the deviations from it), the four stages work on FP32 provisional states, and their
+// tendencies are accumulated into the FP64 state in the reference's order.  Afterwards the
+// module holds the new state, its reconstruction and (lazily) its FP64 diagnostics, as after
+// sw_rk4.
+void Engine::forward(int prec, int nsteps) {
+  if (prec == 0) {
+    rk4(nsteps);
+    return;
+  }
+  if (prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+  if (nsteps < 0) throw EngineError(MPSW_ERR_ARG, "nsteps must be >= 0");
+  prepare();
+  const Phys<double> ph64 = phys();
+  Phys<float> ph{};
+  ph.dt = (float)ph64.dt; ph.apvm = (float)ph64.apvm; ph.visc2 = (float)ph64.visc2; ph.visc4 = (float)ph64.visc4;
+  ph.wind = ph64.wind; ph.drag = ph64.drag; ph.tc1 = ph64.tc1; ph.sphere = ph64.sphere;
+  double w[4], c[4];
+  rk_coeffs(ph64.dt, w, c);
+  double *u0 = dv("u"), *h0 = dv("h");
+  // reference depth: the mean of h(1), rounded to a whole metre (exact in FP32)
+  staging.resize(nC);
+  cuda_check(cudaMemcpyAsync(staging.data(), h0, sizeof(double) * nC, cudaMemcpyDeviceToHost, stream), "h download");
+  cuda_check(cudaStreamSynchronize(stream), "h download");
+  double sum = 0;
+  for (int i = 0; i < nC; i++) sum += staging[i];
+  const double off = nC ? std::round(sum / nC) : 0.0;
+  const float offf = (float)off;
+  using L32 = Launch<float, double>;
+  auto step = [&]() {
+    convert_d2f(nE, u0, s32_u[0], stream);
+    convert_d2f_off(nC, h0, off, s32_h[0], stream);
+    for (int k = 0; k < 4; k++) {
+      const float *ui = s32_u[k], *hi = s32_h[k];
+      RK<float, double> ru{u0, k == 0 ? u0 : acc_u, k == 3 ? u0 : acc_u, k < 3 ? s32_u[k + 1] : nullptr, c[k], w[k], 0.f, ph.tc1};
+      RK<float, double> rh{h0, k == 0 ? h0 : acc_h, k == 3 ? h0 : acc_h, k < 3 ? s32_h[k + 1] : nullptr, c[k], w[k], offf, 0};
+      L32::fwd_vertex(m32, ui, hi, offf, d32, stream);
+      L32::fwd_cell(m32, ui, hi, offf, d32, rh, nullptr, stream);
+      L32::fwd_edge_diag(m32, ui, hi, offf, d32, ph, stream);
+      if (ph.visc4 > 0.f) L32::del4_vc(m32, 1, d32.dsq_u, d32.dsq_vort, d32.dsq_div, stream);
+      L32::fwd_edge_tend(m32, ui, hi, offf, d32, ph, ru, nullptr, stream);
+    }
+  };
+  GraphKey key = graph_key(9, 1, 1, u0, h0);
+  std::memcpy(&key.n2, &off, sizeof(off));
+  for (int n = 0; n < nsteps; n++) run_graph(key, step);
+  finish_levels({"u", "h"});
+  L64::recon(m64, 1, ph64.sphere, u0, dv("uReconstructX"), dv("uReconstructY"), dv("uReconstructZ"),
+             dv("uReconstructZonal"), dv("uReconstructMeridional"), stream);
+  check_launch("forward");
+  for (const char *n : {"u", "h"}) mark_written(var(n), true);
   mark_recon(0);
   mark_diag(0, true);
   pending_diag = 1;
@@ -980,6 +1057,16 @@ int mpsw_var_allocation_tlm(mpsw_handle *h) { return mpsw::guarded(h, [&](mpsw::
 int mpsw_var_allocation_adj(mpsw_handle *h) { return mpsw::guarded(h, [&](mpsw::Engine &e) { e.allocate_group(2); }); }
 int mpsw_sw_mpas_init_block(mpsw_handle *h) { return mpsw::guarded(h, [&](mpsw::Engine &e) { e.init_block(); }); }
 
+int mpsw_get_stream(mpsw_handle *h, void **stream) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) {
+    if (!stream) throw mpsw::EngineError(MPSW_ERR_ARG, "null stream pointer");
+    e.need_device();
+    *stream = (void *)e.stream;
+  });
+}
+int mpsw_forward(mpsw_handle *h, int precision, int nsteps) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.forward(precision, nsteps); });
+}
 int mpsw_sw_rk4(mpsw_handle *h, int nsteps) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) {
     if (nsteps < 0) throw mpsw::EngineError(MPSW_ERR_ARG, "nsteps < 0");

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdlib>
 #include <initializer_list>
 #include <map>
 #include <stdexcept>
@@ -11,6 +13,7 @@
 #include <vector>
 
 #include "mpsw_internal.h"
+#include "mpsw_launch.h"
 #include "mpsw_setup.h"
 
 namespace mpsw {
@@ -122,6 +125,8 @@ struct Engine {
   double *acc_u = nullptr, *acc_h = nullptr, *tacc_u = nullptr, *tacc_h = nullptr;
   AdWork<double> adw{};
   double *tu_[2] = {}, *th_[2] = {}, *xacc_u = nullptr, *xacc_h = nullptr;
+  Diag<float> d32{};                          // FP32-stencil forward (precision 1)
+  float *s32_u[4] = {}, *s32_h[4] = {};
   int pending_diag = 0;  // 1: diagnostics of the level-1 state owed, 2: and their tangents
   Phys<double> phys_cache{};  // physics scalars, refreshed whenever a scalar is assigned
   void refresh_phys();
@@ -176,6 +181,7 @@ struct Engine {
   // module subroutines
   void init_block();
   void rk4(int nsteps);
+  void forward(int prec, int nsteps);
   void rk4_tlm(int nsteps);
   void rk4_adj();
   void solve_diagnostics(int tl);
@@ -206,6 +212,51 @@ struct Engine {
   void to_internal(int kind, int B, const double *src, double *dst, cudaStream_t s);
   void to_reference(int kind, int B, const double *src, double *dst, cudaStream_t s);
 };
+
+// Run `body` (kernel launches on the engine stream, no allocation, no synchronisation) as a
+// CUDA graph: captured on first use for this key, replayed afterwards.  MPSW_GRAPHS=0 runs it
+// eagerly instead.
+constexpr size_t kMaxGraphs = 24;  // captured graphs kept per engine
+
+template <typename F>
+inline void Engine::run_graph(const GraphKey &k, F &&body) {
+  static const bool enabled = !(getenv("MPSW_GRAPHS") && atoi(getenv("MPSW_GRAPHS")) == 0);
+  if (!enabled) {
+    body();
+    return;
+  }
+  for (size_t i = 0; i < graphs.size(); i++)
+    if (graphs[i].key == k) {
+      if (i + 1 < graphs.size()) std::rotate(graphs.begin() + i, graphs.begin() + i + 1, graphs.end());
+      GraphEntry &g = graphs.back();  // most recently used last
+      cuda_check(cudaGraphLaunch(g.exec, stream), "cudaGraphLaunch");
+      g_launches += g.kernels;
+      return;
+    }
+  if (graphs.size() >= kMaxGraphs) {  // evict the least recently used
+    cudaGraphExecDestroy(graphs.front().exec);
+    graphs.erase(graphs.begin());
+  }
+  cudaGraph_t graph = nullptr;
+  const long long before = g_launches;
+  cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
+  GraphEntry e;
+  e.key = k;
+  e.kernels = g_launches - before;  // counted once here, then once per replay
+  const cudaError_t st = cudaGraphInstantiate(&e.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(st, "cudaGraphInstantiate");
+  graphs.push_back(e);
+  cuda_check(cudaGraphLaunch(e.exec, stream), "cudaGraphLaunch");
+}
 
 }  // namespace mpsw
 

@@ -22,6 +22,11 @@ void convert_f2d(long long n, const float *src, double *dst, cudaStream_t s) {
   launch_k(k_convert<float, double>, launch_cfg(n), s, n, src, dst);
 }
 
+void convert_d2f_off(long long n, const double *src, double off, float *dst, cudaStream_t s) {
+  g_launches++;
+  launch_k(k_convert_off, launch_cfg(n), s, n, src, off, dst);
+}
+
 void convert_list(const ConvList &L, long long max_n, cudaStream_t s) {
   g_launches++;
   launch_k(k_convert_list, launch_cfg(max_n), s, L);

@@ -309,6 +309,11 @@ __global__ void k_convert(long long n, const S *__restrict__ src, D *dst) {
 }
 
 // Rounds up to kConvMax double arrays to float in one launch (linearisation point of a stage).
+// dst = float(src - off): reduced-precision h relative to a reference depth
+static __global__ void k_convert_off(long long n, const double *src, double off, float *dst) {
+  MPSW_GRID_LOOP(t, n) dst[t] = float(src[t] - off);
+}
+
 static __global__ void k_convert_list(ConvList L) {
   pdl_begin();  // also when the list is empty
   for (int i = 0; i < L.count; i++) {

@@ -55,6 +55,7 @@ struct Launch {
 };
 
 void convert_d2f(long long n, const double *src, float *dst, cudaStream_t s);
+void convert_d2f_off(long long n, const double *src, double off, float *dst, cudaStream_t s);
 void convert_list(const ConvList &L, long long max_n, cudaStream_t s);
 void convert_f2d(long long n, const float *src, double *dst, cudaStream_t s);
 

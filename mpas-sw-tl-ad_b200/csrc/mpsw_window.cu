@@ -167,51 +167,6 @@ GraphKey Engine::graph_key(int kind, int prec, int B, const void *p1, const void
   return k;
 }
 
-// Run `body` (kernel launches on the engine stream, no allocation, no synchronisation) as a
-// CUDA graph: captured on first use for this key, replayed afterwards.  MPSW_GRAPHS=0 runs it
-// eagerly instead.
-constexpr size_t kMaxGraphs = 24;
-
-template <typename F>
-void Engine::run_graph(const GraphKey &k, F &&body) {
-  static const bool enabled = !(getenv("MPSW_GRAPHS") && atoi(getenv("MPSW_GRAPHS")) == 0);
-  if (!enabled) {
-    body();
-    return;
-  }
-  for (size_t i = 0; i < graphs.size(); i++)
-    if (graphs[i].key == k) {
-      if (i + 1 < graphs.size()) std::rotate(graphs.begin() + i, graphs.begin() + i + 1, graphs.end());
-      GraphEntry &g = graphs.back();  // most recently used last
-      cuda_check(cudaGraphLaunch(g.exec, stream), "cudaGraphLaunch");
-      g_launches += g.kernels;
-      return;
-    }
-  if (graphs.size() >= kMaxGraphs) {  // evict the least recently used
-    cudaGraphExecDestroy(graphs.front().exec);
-    graphs.erase(graphs.begin());
-  }
-  cudaGraph_t graph = nullptr;
-  const long long before = g_launches;
-  cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-  try {
-    body();
-  } catch (...) {
-    cudaStreamEndCapture(stream, &graph);
-    if (graph) cudaGraphDestroy(graph);
-    throw;
-  }
-  cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
-  GraphEntry e;
-  e.key = k;
-  e.kernels = g_launches - before;  // counted once here, then once per replay
-  const cudaError_t st = cudaGraphInstantiate(&e.exec, graph, 0);
-  cudaGraphDestroy(graph);
-  cuda_check(st, "cudaGraphInstantiate");
-  graphs.push_back(e);
-  cuda_check(cudaGraphLaunch(e.exec, stream), "cudaGraphLaunch");
-}
-
 void Engine::window_free() {
   Window &W = win;
   graphs_free();

@@ -204,6 +204,19 @@ class MpasSwModule:
             tr[1] = tr[0]
         self.rk_step = 5
 
+    def sw_rk4_steps(self, nsteps, precision=0):
+        """``nsteps`` calls of sw_rk4 in one device call (no counterpart in the reference).
+        precision 0 is bit-identical to repeated sw_rk4; precision 1 runs the stencils in FP32
+        and keeps the state and its RK4 accumulation in FP64 (tend_u / tend_h are then left
+        as they were)."""
+        self._run('mpsw_forward', int(precision), int(nsteps), reads=_STATE, eager=_STATE,
+                  lazy=_DIAG + (('tend_u', 'tend_h') if int(precision) == 0 else ()))
+        tr = self.__dict__['_arr'].get('tracers')
+        if tr is not None and nsteps > 0:
+            tr[1] = tr[0]
+        if nsteps > 0:
+            self.rk_step = 5
+
     def sw_rk4_tlm(self):
         self._run('mpsw_sw_rk4_tlm', 1, reads=_STATE + _sfx(_STATE, '_tl'),
                   eager=_STATE + _sfx(_STATE, '_tl'),
