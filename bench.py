@@ -457,6 +457,7 @@ def run_mpsw(a, rank, world):
                        'stage_storage': {-1: 'auto (FP64+FP32 stage linearisation points when they fit 40%% of free HBM)', 0: 'none: stages recomputed from checkpoints', 1: 'FP64', 2: 'FP32', 3: 'FP64+FP32'}[a.storage],
                        'members_per_gpu': B, 'parallelism': 'replicas x%d' % world,
                        'l2': 'flushed (256 MB write) between timed steps; working set ~%.0f MB' % wset},
+            'step_ms': [round(t, 3) for t in t32],
             'phase_ms': phases,
             'fp64_plain_gradients_per_s': plain,
             'batched_vs_plain': (value / world / plain) if plain else None,

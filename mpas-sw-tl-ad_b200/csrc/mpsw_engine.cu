@@ -355,6 +355,7 @@ void Engine::fill_mesh(MeshDev<R> &m) {
   m.c_eoc = up<int>(bm.c_eoc, o);
   m.c_es = up<int>(bm.c_es, o);
   m.c_esg = up<signed char>(bm.c_esg, o);
+
   m.c_vs = up<int>(bm.c_vs, o);
   m.c_vk = up<R>(bm.c_vk, o);
   m.c_area = up<R>(bm.c_area, o);
@@ -445,6 +446,17 @@ void Engine::build_device_mesh() {
   free_device_mesh();
   fill_mesh(m64);
   fill_mesh(m32);
+  {  // the cell across each edge of a cell, in the order of c_es
+    std::vector<int> nb(bm.c_es.size(), 0);
+    for (int k = 0; k < MAXE; k++)
+      for (int c = 0; c < bm.nC; c++) {
+        const size_t i = (size_t)k * bm.nC + c;
+        if (k >= bm.c_n[c]) continue;
+        const int e = bm.c_es[i];
+        nb[i] = bm.e_c1[e] == c ? bm.e_c2[e] : bm.e_c1[e];
+      }
+    d_cnb = up<int>(nb, mesh_bufs);
+  }
   d_perm[0] = up<int>(bm.perm_c, mesh_bufs);
   d_perm[1] = up<int>(bm.perm_e, mesh_bufs);
   d_perm[2] = up<int>(bm.perm_v, mesh_bufs);
@@ -567,7 +579,7 @@ using L64 = Launch<double, double>;
 void Engine::fwd_diag(const double *u, const double *h, const Diag<double> &d, const Phys<double> &ph) {
   RK<double, double> none{};
   L64::fwd_vertex(m64, u, h, 0.0, d, stream);
-  L64::fwd_cell(m64, u, h, 0.0, d, none, nullptr, stream);
+  L64::fwd_cell(m64, d_cnb, u, h, 0.0, d, none, nullptr, stream);
   L64::fwd_edge_diag(m64, u, h, 0.0, d, ph, stream);
   if (ph.visc4 > 0) L64::del4_vc(m64, 1, d.dsq_u, d.dsq_vort, d.dsq_div, stream);
 }
@@ -575,7 +587,7 @@ void Engine::fwd_diag(const double *u, const double *h, const Diag<double> &d, c
 void Engine::fwd_stage(const double *u, const double *h, const Diag<double> &d, const Phys<double> &ph,
                        const RK<double, double> &rku, const RK<double, double> &rkh, double *tu, double *th) {
   L64::fwd_vertex(m64, u, h, 0.0, d, stream);
-  L64::fwd_cell(m64, u, h, 0.0, d, rkh, th, stream);
+  L64::fwd_cell(m64, d_cnb, u, h, 0.0, d, rkh, th, stream);
   L64::fwd_edge_diag(m64, u, h, 0.0, d, ph, stream);
   if (ph.visc4 > 0) L64::del4_vc(m64, 1, d.dsq_u, d.dsq_vort, d.dsq_div, stream);
   L64::fwd_edge_tend(m64, u, h, 0.0, d, ph, rku, tu, stream);
@@ -728,7 +740,7 @@ void Engine::forward(int prec, int nsteps) {
       RK<float, double> ru{u0, k == 0 ? u0 : acc_u, k == 3 ? u0 : acc_u, k < 3 ? s32_u[k + 1] : nullptr, c[k], w[k], 0.f, ph.tc1};
       RK<float, double> rh{h0, k == 0 ? h0 : acc_h, k == 3 ? h0 : acc_h, k < 3 ? s32_h[k + 1] : nullptr, c[k], w[k], offf, 0};
       L32::fwd_vertex(m32, ui, hi, offf, d32, stream);
-      L32::fwd_cell(m32, ui, hi, offf, d32, rh, nullptr, stream);
+      L32::fwd_cell(m32, d_cnb, ui, hi, offf, d32, rh, nullptr, stream);
       L32::fwd_edge_diag(m32, ui, hi, offf, d32, ph, stream);
       if (ph.visc4 > 0.f) L32::del4_vc(m32, 1, d32.dsq_u, d32.dsq_vort, d32.dsq_div, stream);
       L32::fwd_edge_tend(m32, ui, hi, offf, d32, ph, ru, nullptr, stream);

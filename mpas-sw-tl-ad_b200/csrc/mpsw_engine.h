@@ -115,6 +115,7 @@ struct Engine {
   MeshDev<float> m32{};
   std::vector<void *> mesh_bufs;
   const int *d_perm[3] = {nullptr, nullptr, nullptr};
+  const int *d_cnb = nullptr;  // [MAXE][nCells] the cell across each edge of a cell
 
   // work
   std::vector<void *> work;

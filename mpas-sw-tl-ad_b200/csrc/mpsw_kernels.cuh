@@ -37,6 +37,24 @@ __device__ __forceinline__ R ld(const R *p, size_t i) {
   return __ldg(p + i);
 }
 
+// Bounds of the neighbour loops.  BoundsNarrow serves meshes with at most 10 edgesOnEdge and 6
+// edgesOnCell (every quasi-uniform hexagon/pentagon mesh): the loops get compile-time trip
+// counts and are unrolled with `slot < n` as a predicate, so the connectivity, weight and member
+// loads of all slots can be in flight together instead of one slot after another.  BoundsAny
+// keeps runtime trip counts for any mesh within MAXE2 / MAXE.
+struct BoundsNarrow {
+  static constexpr int e2 = 10, c = 6;
+};
+struct BoundsAny {
+  static constexpr int e2 = 0, c = 0;
+};
+
+// j over the first n slots of a list whose length is at most NMAX (NMAX 0: no static bound)
+#define MPSW_SLOTS(j, NMAX, n)                                                \
+  _Pragma("unroll") for (int j = 0; j < ((NMAX) > 0 ? (NMAX) : (n)); j++) \
+    if ((NMAX) == 0 || j < (n))
+
+
 // ----------------------------------------------------------------------------------------
 // Forward: sw_compute_solve_diagnostics (src/mpas_sw_dyncore.f90:1-361) split by entity.
 // h is stored relative to `off` (0 for FP64, a reference depth for reduced precision).
@@ -73,20 +91,23 @@ __global__ void k_fwd_vertex(MeshDev<R> m, const R *__restrict__ u, const R *__r
 
 // divergence (:222-242), ke (:245-256), pv_cell/vorticity_cell (:324-340) and the thickness
 // tendency (:468-482) with its RK update.
+// c_nb[k][c] is the cell across edge k of the cell (its h_edge sums this cell's h and that
+// cell's, in either order: the same value)
 template <typename R, typename A>
-__global__ void k_fwd_cell(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ h, R off,
-                           Diag<R> d, RK<R, A> rk, R *tend_h) {
+__global__ void k_fwd_cell(MeshDev<R> m, const int *__restrict__ c_nb, const R *__restrict__ u,
+                           const R *__restrict__ h, R off, Diag<R> d, RK<R, A> rk, R *tend_h) {
   const int nC = m.nC;
   MPSW_GRID_LOOP(t, nC) {
     const int c = (int)t;
     const int n = ld(m.c_n, c);
+    const R hc = ld(h, c) + off;
     R div = R(0), th = R(0);
     for (int k = 0; k < n; k++) {
       const int e = ld(m.c_es, (size_t)k * nC + c);
       const R s = R(m.c_esg[(size_t)k * nC + c]);
       const R ue = ld(u, e), dve = ld(m.e_dv, e);
       div = div + s * (ue * dve);
-      const R he = R(0.5) * ((ld(h, ld(m.e_c1, e)) + off) + (ld(h, ld(m.e_c2, e)) + off));
+      const R he = R(0.5) * (hc + (ld(h, ld(c_nb, (size_t)k * nC + c)) + off));
       th = th + (-s) * ((ue * dve) * he);
     }
     const R area = ld(m.c_area, c);

@@ -124,10 +124,10 @@ void Launch<R, A>::fwd_vertex(const MeshDev<R> &m, const R *u, const R *h, R off
   launch_k(k_fwd_vertex<R>, launch_cfg(m.nV), s, m, u, h, off, d);
 }
 template <typename R, typename A>
-void Launch<R, A>::fwd_cell(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
-                            const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
+void Launch<R, A>::fwd_cell(const MeshDev<R> &m, const int *c_nb, const R *u, const R *h, R off,
+                            const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
-  launch_k(k_fwd_cell<R, A>, launch_cfg(m.nC), s, m, u, h, off, d, rk, tend_h);
+  launch_k(k_fwd_cell<R, A>, launch_cfg(m.nC), s, m, c_nb, u, h, off, d, rk, tend_h);
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,

@@ -16,7 +16,7 @@ template <typename R, typename A>
 struct Launch {
   // forward stage pieces (single trajectory)
   static void fwd_vertex(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d, cudaStream_t s);
-  static void fwd_cell(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
+  static void fwd_cell(const MeshDev<R> &m, const int *c_nb, const R *u, const R *h, R off, const Diag<R> &d,
                        const RK<R, A> &rk, R *tend_h, cudaStream_t s);
   static void fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                             const Phys<R> &ph, cudaStream_t s);

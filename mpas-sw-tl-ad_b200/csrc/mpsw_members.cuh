@@ -90,23 +90,6 @@ __device__ __forceinline__ EntMember ent_member(long long t, int B, int V) {
   return {ent, (int)(t - (long long)ent * bv) * V};
 }
 
-// Bounds of the neighbour loops.  BoundsNarrow serves meshes with at most 10 edgesOnEdge and 6
-// edgesOnCell (every quasi-uniform hexagon/pentagon mesh): the loops get compile-time trip
-// counts and are unrolled with `slot < n` as a predicate, so the connectivity, weight and member
-// loads of all slots can be in flight together instead of one slot after another.  BoundsAny
-// keeps runtime trip counts for any mesh within MAXE2 / MAXE.
-struct BoundsNarrow {
-  static constexpr int e2 = 10, c = 6;
-};
-struct BoundsAny {
-  static constexpr int e2 = 0, c = 0;
-};
-
-// j over the first n slots of a list whose length is at most NMAX (NMAX 0: no static bound)
-#define MPSW_SLOTS(j, NMAX, n)                                                \
-  _Pragma("unroll") for (int j = 0; j < ((NMAX) > 0 ? (NMAX) : (n)); j++) \
-    if ((NMAX) == 0 || j < (n))
-
 // RK4 bookkeeping of V members (src/mpas_sw_module.f90:590-611)
 template <typename R, typename A, int V>
 __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const Mv<R, V> &t) {

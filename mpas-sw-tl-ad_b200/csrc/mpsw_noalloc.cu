@@ -88,7 +88,7 @@ extern "C" int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const 
     using L = Launch<double, double>;
     const RK<double, double> none{};
     L::fwd_vertex(e.m64, u, hh, 0.0, d, s);
-    L::fwd_cell(e.m64, u, hh, 0.0, d, none, tend_h, s);
+    L::fwd_cell(e.m64, e.d_cnb, u, hh, 0.0, d, none, tend_h, s);
     L::fwd_edge_diag(e.m64, u, hh, 0.0, d, ph, s);
     if (ph.visc4 > 0) L::del4_vc(e.m64, 1, d.dsq_u, d.dsq_vort, d.dsq_div, s);
     L::fwd_edge_tend(e.m64, u, hh, 0.0, d, ph, none, tend_u, s);

@@ -8,7 +8,8 @@ import ctypes
 import os
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, 'libmpsw.so')
+# the library built in place by build.py; MPSW_LIB names another build of it
+LIB_PATH = os.environ.get('MPSW_LIB') or os.path.join(PKG_DIR, 'libmpsw.so')
 
 _c_int, _c_double, _vp, _cp, _ll = (ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
                                     ctypes.c_char_p, ctypes.c_longlong)
