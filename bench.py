@@ -37,9 +37,10 @@ def parse():
     p.add_argument('--steps', type=int, default=3)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='mpsw', choices=['mpsw', 'reference'])
-    p.add_argument('--workload', default='tlad', choices=['tlad', 'fwd'],
+    p.add_argument('--workload', default='tlad', choices=['tlad', 'fwd', 'costs'],
                    help='tlad: batched TL+AD gradients (level 5, 288 steps of 300 s, B=64); '
-                        'fwd: nonlinear forward with mountains (level 7, 1152 steps of 75 s), sim-days/s')
+                        'fwd: nonlinear forward with mountains (level 7, 1152 steps of 75 s), sim-days/s; '
+                        'costs: 64 cost-function gradients by one batched adjoint (level 6, 1152 steps of 150 s)')
     p.add_argument('--batch', type=int, default=64)
     p.add_argument('--level', type=int, default=None)
     p.add_argument('--nsteps', type=int, default=None)
@@ -54,7 +55,7 @@ def parse():
     p.add_argument('--profile', action='store_true',
                    help='only the timed batched windows (for profiler launch lists); no JSON line')
     a = p.parse_args()
-    dflt = {'tlad': (5, 288, 300.0), 'fwd': (7, 1152, 75.0)}[a.workload]
+    dflt = {'tlad': (5, 288, 300.0), 'fwd': (7, 1152, 75.0), 'costs': (6, 1152, 150.0)}[a.workload]
     a.level = dflt[0] if a.level is None else a.level
     a.nsteps = dflt[1] if a.nsteps is None else a.nsteps
     a.dt = dflt[2] if a.dt is None else a.dt
@@ -635,6 +636,146 @@ def run_forward(a, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def _oracle_costs_sample(args):
+    """Seconds per step of the oracle's forward and adjoint (one cost function) on the host."""
+    level, dt, n = args
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    unit, mesh, st = workload(level, dt)
+    m = O.OracleModule()
+    load_module(m, unit, mesh, st, dt)
+    m.var_allocation_adj()
+    m.sw_mpas_init_block()
+    u0, h0 = m.u[0, 0].copy(), m.h[0, 0].copy()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        m.sw_rk4()
+    t1 = time.perf_counter()
+    m.h_ad[0, 0] = m.h[0, 0]
+    for _ in range(n):
+        m.u[0, 0], m.h[0, 0] = u0, h0
+        m.sw_rk4_adj()
+    t2 = time.perf_counter()
+    return (t1 - t0) / n, (t2 - t1) / n
+
+
+def run_costs(a, rank, world):
+    """Gradients of B quadratic costs J_k = 1/2 |M_k h(T)|^2 (M_k: seeded spherical-cap masks)
+    with respect to the initial state: one window forward, then one batched adjoint sweep seeded
+    with M_k^T M_k h(T); FP32 stencils with FP64 accumulation, beside sequential plain FP64
+    adjoint runs (one cost per window)."""
+    import ctypes
+    import torch
+    from module_sw_mpas import MpasSwModule
+    from mpsw import _lib, ic, replicas
+    from mpsw.torch_api import FP32, FP64, Engine, Window
+
+    dev = rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    unit, mesh, st = workload(a.level, a.dt)
+    mod = MpasSwModule()
+    load_module(mod, unit, mesh, st, a.dt)
+    mod.var_allocation_adj()
+    mod.sw_mpas_init_block()
+    eng = Engine(mod)
+    L = _lib.load()
+    B = a.batch
+    nC, nE, nV = unit['nCells'], unit['nEdges'], unit['nVertices']
+    masks = torch.tensor(ic.cap_masks(mesh, replicas.member_seed(3, rank), B), device='cuda')
+    masks_i = eng.to_internal(masks, 0)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+
+    def gradients(prec, mk):
+        """One bench step: window forward, seeds from h(T), batched adjoint; internal order."""
+        w = Window(eng, a.nsteps, a.ckpt, a.storage)
+        uT = torch.empty(nE, 1, dtype=torch.float64, device='cuda')
+        hT = torch.empty(nC, 1, dtype=torch.float64, device='cuda')
+        eng.h.call('mpsw_window_final_state', ctypes.c_void_p(uT.data_ptr()), ctypes.c_void_p(hT.data_ptr()),
+                   ctypes.c_void_p(stream.cuda_stream))
+        au = torch.zeros(nE, mk.shape[1], dtype=torch.float64, device='cuda')
+        ah = (mk * mk * hT).contiguous()
+        w.ad_internal(au, ah, prec)
+        return au, ah
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def timed(fn, n_warm, n_time):
+        for _ in range(n_warm):
+            fn()
+        times = []
+        launches0 = L.mpsw_launch_count()
+        for _ in range(n_time):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            barrier()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            times.append(e0.elapsed_time(e1))
+        return times, (L.mpsw_launch_count() - launches0) / n_time
+
+    with Clocks(dev) as clk:
+        t32, launches = timed(lambda: gradients(FP32, masks_i), a.warmup, a.steps)
+    clocks = clk.summary()
+    ms = replicas.max_over_ranks(sum(t32) / len(t32), device='cuda')
+    value = world * B / (ms / 1e3)
+    gu32, gh32 = gradients(FP32, masks_i)
+    gu64, gh64 = gradients(FP64, masks_i)
+    num = torch.sqrt(((gu32 - gu64) ** 2).sum(0) + ((gh32 - gh64) ** 2).sum(0))
+    den = torch.sqrt((gu64 ** 2).sum(0) + (gh64 ** 2).sum(0))
+    rel_err = float((num / den).max())
+    # sequential plain FP64 adjoint runs: one cost per window
+    tp, _ = timed(lambda: gradients(FP64, masks_i[:, :1].contiguous()), 1, 1)
+    seq = 1.0 / (tp[0] / 1e3)
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json')))
+    except Exception:
+        pass
+    hbm = peaks.get('hbm_gbs') or 6650.0
+    gradients(FP32, masks_i)  # leaves the buffers of this configuration in place
+    out = ctypes.c_double()
+    eng.h.check(L.mpsw_time_kernel(eng.h.ptr, 9, FP32, B, 10, ctypes.byref(out)), 'time_kernel')
+    sum_eoe = int(unit['nEdgesOnEdge'].sum())
+    sb = kernel_bytes('ad_stage', nC, nE, nV, sum_eoe, B, 4)
+    ach = sb / (out.value / 1e3) / 1e9
+    cpu = None
+    if rank == 0:
+        sample = 3
+        f, adj = _oracle_costs_sample((a.level, a.dt, sample))
+        cpu = {'value': 1.0 / ((f + adj) * a.nsteps), 'unit': 'gradients/s', 'cores': 1, 'kind': 'port',
+               'sample': '%d forward + %d adjoint steps of the oracle (one cost), extrapolated to %d steps' % (sample, sample, a.nsteps)}
+    if rank == 0:
+        line = {
+            'metric': 'cost-function gradients/s, batched FP32 adjoint vs sequential plain FP64 (rel err<=1e-4)',
+            'value': value, 'unit': 'gradients/s', 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
+            'ms_per_step': ms, 'step_ms': [round(t, 3) for t in t32], 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32 stencils + f64 accumulation',
+            'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh, %d seeded spherical-cap masks)' % (a.level, B),
+            'config': {'workload': 'costs: level-%d mesh (%d cells), %d RK4 steps of %g s, %d costs J_k = 1/2 |M_k h(T)|^2' % (a.level, nC, a.nsteps, a.dt, B),
+                       'parallelism': 'replicas x%d' % world, 'l2': 'flushed (256 MB write) between timed steps'},
+            'sequential_fp64_gradients_per_s': seq,
+            'batched_vs_sequential': value / world / seq,
+            'rel_err_fp32_vs_fp64': rel_err,
+            'roofline': {'bound': 'hbm', 'kernel': 'one adjoint stage (ad_edge, ad_cell, ad_vertex, ad_final)',
+                         'achieved': ach, 'peak': hbm, 'unit': 'GB/s', 'frac': ach / hbm, 'traffic': None,
+                         'algorithmic_bytes': sb, 'ms_per_launch': out.value,
+                         'peak_source': 'measured' if peaks.get('hbm_gbs') else 'fallback'},
+            'cpu_baseline': cpu,
+            'clocks': clocks,
+            'gpu_launches': int(launches),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get('RANK', '0'))
@@ -650,6 +791,8 @@ def main():
         run_reference(a, rank, world)
     elif a.workload == 'fwd':
         run_forward(a, rank, world)
+    elif a.workload == 'costs':
+        run_costs(a, rank, world)
     else:
         run_mpsw(a, rank, world)
     if world > 1 and a.impl == 'mpsw':
