@@ -233,9 +233,10 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
 
     s: bytes of a member value, a linearisation-point value and a mesh metric (4 in FP32);
     accumulators and member RK states are a = 8 bytes; connectivity words 4 bytes, edge signs
-    1 byte.  E, C, V: edges, cells, vertices.  As mpsw_time_kernel launches them, the RK state
-    x0 and the accumulator are one FP64 array, so RK bookkeeping reads it, writes it and writes
-    the next provisional state (2a + s per member value); ad_final's x2 is that array too."""
+    1 byte.  E, C, V: edges, cells, vertices.  RK bookkeeping of a middle stage, as the sweeps
+    and mpsw_time_kernel run it, reads the FP64 state x0 and writes the next provisional state
+    and the stage's tendency (a + 2s per member value); ad_final reads x2 and writes the next
+    tendency adjoint and its stage contribution (a + 2s)."""
     a, i, E, C, V, S = 8, 4, nE, nC, nV, sum_eoe
     eoe = i * (E + S) + s * S                              # nEdgesOnEdge, edgesOnEdge, weights
     kb = {
@@ -244,11 +245,11 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
                      + B * s * (E + C + 2 * V),                           # u,h in; vort, pv out
         'tl_cell': (i + 3 * 6 * i + 6 + 6 * s + s) * C + (2 * i + 2 * s) * E  # c_n,es,eoc,vs,esg,kites,area; c1,c2,dc,dv
                    + 2 * s * E                                                  # base u, h_edge
-                   + B * (s * (E + C + V + 3 * C) + (2 * a + s) * C),          # u,h,pv in; div,ke,pc out; RK
+                   + B * (s * (E + C + V + 3 * C) + (a + 2 * s) * C),          # u,h,pv in; div,ke,pc out; RK
         'tl_edge_diag': eoe + (6 * i + 2 * s) * E + 4 * s * E                  # ends; dc,dv; base gradPVt,v,gradPVn,u
                         + B * s * (E + C + V + C + 2 * E),                     # u,h,pv,pc in; pv_edge,h_edge out
         'tl_edge_tend': eoe + (2 * i + s) * E + 3 * s * E                      # c1,c2,dc; base pv_edge,u,h_edge
-                        + B * (s * (3 * E + 2 * C) + (2 * a + s) * E),         # u,pe,he,ke,h in; RK
+                        + B * (s * (3 * E + 2 * C) + (a + 2 * s) * E),         # u,pe,he,ke,h in; RK
         'ad_edge': eoe + s * S + (2 * i + s) * E + 6 * s * E                   # wrev; c1,c2,dv; 6 base fields
                    + B * s * (E + C + 6 * E),                                  # tu,th in; 6 adjoints out
         'ad_cell': (i + 6 * i + 6 + s) * C + s * E                             # c_n,es,esg,area; dc
@@ -256,7 +257,7 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
         'ad_vertex': (3 * i + 3 * s + 3 * i + 3 * i + 3 + 2 * s) * V + s * C + s * E + 2 * s * V
                      + B * s * (C + 2 * E + 2 * V),                            # pc_ad,pe_ad,gpt_ad in; 2 out
         'ad_final': (i + 6 * i + 6 * s + s) * C + i * (E + S) + s * S + (4 * i + 2 * s) * E + s * E
-                    + B * (s * (2 * C + 2 * V + 2 * E + C) + (2 * a + s) * (C + E)),
+                    + B * (s * (2 * C + 2 * V + 2 * E + C) + (a + 2 * s) * (C + E)),
     }
     kb['tl_stage'] = sum(kb[k] for k in ('tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend'))
     kb['ad_stage'] = sum(kb[k] for k in ('ad_edge', 'ad_cell', 'ad_vertex', 'ad_final'))

@@ -103,6 +103,12 @@ struct RK {
   A c, w;
   R off;      // next stores x - off (reference-depth offset of the reduced-precision h)
   int frozen; // test case 1: the wind stays at x0
+  // Deferred accumulation (member sweeps): stages 1-3 store their tendency in t_out instead of
+  // accumulating; the last stage (t_in[0] set) writes acc_out = (((x0 + wt[0] t_in[0]) +
+  // wt[1] t_in[1]) + wt[2] t_in[2]) + w t, the same FP64 operations as accumulating stage by stage.
+  R *t_out;
+  const R *t_in[3];
+  A wt[3];
 };
 
 // Input of one adjoint stage: its tendency adjoint, tu (edges) and th / areaCell (cells), as
@@ -145,6 +151,11 @@ struct AdOut {
   int mode;
   R *tu_next, *th_next;
   A wu, cu, wh, ch;
+  // Deferred accumulation (member sweeps): instead of adding into acc, AD_SET / AD_ADD stages
+  // store their contribution in pad_out_*, and AD_FINAL (pad_in_*[0] set) sums the three stored
+  // contributions in stage order before adding x2 and its own: the same FP64 operations.
+  R *pad_out_u, *pad_out_h;
+  const R *pad_in_u[3], *pad_in_h[3];
 };
 
 // Up to kConvMax double arrays rounded to float by one launch (see convert_list).

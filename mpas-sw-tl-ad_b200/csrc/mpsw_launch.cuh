@@ -60,16 +60,17 @@ inline void launch_k(void (*kernel)(KArgs...), LaunchCfg c, cudaStream_t s, Args
 extern long long g_launches;
 
 // Members per thread of a member kernel: 16 bytes of R per vector load (4 floats, 2 doubles),
-// reduced while B is not a multiple of it or a buffer is not aligned to V elements of the wider
-// of R and A.  MPSW_VEC=1|2|4 overrides the starting width.
+// or `prefer` (a kernel measured faster at another width), reduced while B is not a multiple of
+// it or a buffer is not aligned to V elements of the wider of R and A.  MPSW_VEC=1|2|4|8 overrides the starting width (8: FP32 only).
 template <typename R, typename A>
-inline int vec_width(int B, std::initializer_list<const void *> ptrs) {
+inline int vec_width(int B, std::initializer_list<const void *> ptrs, int prefer = 0) {
   static const int forced = [] {
     const char *e = std::getenv("MPSW_VEC");
     const int v = e ? std::atoi(e) : 0;
-    return (v == 1 || v == 2 || v == 4) ? v : 0;
+    return (v == 1 || v == 2 || v == 4 || v == 8) ? v : 0;
   }();
-  int v = forced ? forced : (int)(16 / sizeof(R));
+  int v = forced ? forced : prefer ? prefer : (int)(16 / sizeof(R));
+  if (sizeof(R) > 4 && v > 4) v = 4;  // 8 members per thread: FP32 only
   const size_t wide = sizeof(R) > sizeof(A) ? sizeof(R) : sizeof(A);
   for (; v > 1; v >>= 1) {
     if (B % v) continue;
@@ -100,6 +101,11 @@ inline LaunchCfg staged_cfg(int n, int B, int v, size_t smem_per_edge_bytes) {
   return {(n + epb - 1) / epb, epb * tpe, smem_per_edge_bytes * epb};
 }
 
+// Width for the kernels measured faster at 8 FP32 members per thread (tl_edge_diag, ad_final):
+// 0 (the default width) in FP64.
+template <typename R>
+constexpr int kWideV = sizeof(R) == 4 ? 8 : 0;
+
 // run the statement with NB = BoundsNarrow when the mesh allows it, else BoundsAny
 #define MPSW_BDISPATCH(m, ...)                                  \
   if ((m).max_eoe <= BoundsNarrow::e2 && (m).max_eoc <= BoundsNarrow::c) { \
@@ -112,6 +118,7 @@ inline LaunchCfg staged_cfg(int n, int B, int v, size_t smem_per_edge_bytes) {
 
 #define MPSW_VDISPATCH(v, ...)                            \
   switch (v) {                                            \
+    case 8: { constexpr int VV = 8; if constexpr (sizeof(R) == 4) { __VA_ARGS__; } } break; \
     case 4: { constexpr int VV = 4; __VA_ARGS__; } break;  \
     case 2: { constexpr int VV = 2; __VA_ARGS__; } break;  \
     default: { constexpr int VV = 1; __VA_ARGS__; } break; \
@@ -173,7 +180,7 @@ void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const 
                            const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.div, d.ke, d.pc, d.vc, d.pvv, d.vort, tend_h, rk.x0, rk.acc_in,
-                                    rk.acc_out, rk.next});
+                                    rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1], rk.t_in[2]});
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_cell<R, A, VV, NB>, launch_cfg((long long)(m.nC) * ((B) / (VV))), s, m, B, bs, ut, ht, d, rk, tend_h)));
 }
 template <typename R, typename A>
@@ -182,7 +189,8 @@ void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, c
   g_launches++;
   Diag<R> dd = d;
   if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
-  const int v = vec_width<R, A>(B, {ut, ht, dd.pvv, dd.pc, dd.div, dd.vort, dd.pe, dd.he, dd.v, dd.gpt, dd.gpn, dd.dsq_u});
+  const int v = vec_width<R, A>(B, {ut, ht, dd.pvv, dd.pc, dd.div, dd.vort, dd.pe, dd.he, dd.v, dd.gpt, dd.gpn, dd.dsq_u},
+                                kWideV<R>);
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, dd, ph)));
 }
 template <typename R, typename A>
@@ -191,7 +199,8 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
                                 cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
-                                    rk.x0, rk.acc_in, rk.acc_out, rk.next});
+                                    rk.x0, rk.acc_in, rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1],
+                                    rk.t_in[2]});
   constexpr int J = BoundsNarrow::e2;
   if (use_staged(m, B, v, eoe_stage_bytes<R, J, 3>(1))) {
     MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eoe_stage_bytes<R, J, 3>(1)),
@@ -202,10 +211,13 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
 }
 // members per thread of one adjoint stage: every buffer the five kernels touch
 template <typename R, typename A>
-static int ad_width(int B, const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out) {
+static int ad_width(int B, const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out, int prefer = 0) {
   return vec_width<R, A>(B, {in.tu, in.th, w.pe_ad, w.he_ad, w.ud, w.gpn_ad, w.gpt_ad, w.v_ad, w.du_ad, w.pc_ad,
                              w.ke_ad, w.div_ad, w.hd, w.dd_ad, w.hv_ad, w.circ_ad, w.dc_ad, out.acc_u, out.acc_h,
-                             out.x2u, out.x2h, out.dst_u, out.dst_h, out.tu_next, out.th_next});
+                             out.x2u, out.x2h, out.dst_u, out.dst_h, out.tu_next, out.th_next, out.pad_out_u,
+                             out.pad_out_h, out.pad_in_u[0], out.pad_in_u[1], out.pad_in_u[2], out.pad_in_h[0],
+                             out.pad_in_h[1], out.pad_in_h[2]},
+                         prefer);
 }
 
 template <typename R, typename A, int V, class NB>
@@ -236,8 +248,9 @@ void Launch<R, A>::ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const
     }
     ad_launch<R, A, VV, NB>(1, m, B, bs, ph, in, sd, w, out, s);
     ad_launch<R, A, VV, NB>(2, m, B, bs, ph, in, sd, w, out, s);
-    ad_launch<R, A, VV, NB>(3, m, B, bs, ph, in, sd, w, out, s);
   }));
+  const int vf = ad_width<R, A>(B, in, w, out, kWideV<R>);  // ad_final runs wider
+  MPSW_VDISPATCH(vf, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(3, m, B, bs, ph, in, sd, w, out, s)));
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
@@ -245,7 +258,9 @@ void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> 
                            cudaStream_t s) {
   const AdSeeds<R> sd{};
   const int v = ad_width<R, A>(B, in, w, out);
-  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(which < 0 || which > 3 ? 3 : which, m, B, bs, ph, in, sd, w, out, s)));
+  const int k = which < 0 || which > 3 ? 3 : which;
+  const int vk = k == 3 ? ad_width<R, A>(B, in, w, out, kWideV<R>) : v;
+  MPSW_VDISPATCH(vk, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(k, m, B, bs, ph, in, sd, w, out, s)));
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,

@@ -100,7 +100,21 @@ __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const M
     for (int i = 0; i < V; i++) n.x[i] = rk.frozen ? R(x0.x[i]) : R(x0.x[i] + rk.c * A(t.x[i]));
     stv<V>(rk.next + o, n);
   }
-  if (rk.acc_out && !rk.frozen) {
+  if (rk.frozen) return;
+  if (rk.t_out) {
+    stv<V>(rk.t_out + o, t);
+  } else if (rk.t_in[0]) {
+    Mv<A, V> a = ldv<V>(rk.x0 + o);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const Mv<R, V> tj = ldv<V>(rk.t_in[j] + o);
+#pragma unroll
+      for (int i = 0; i < V; i++) a.x[i] = a.x[i] + rk.wt[j] * A(tj.x[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < V; i++) a.x[i] = a.x[i] + rk.w * A(t.x[i]);
+    stv<V>(rk.acc_out + o, a);
+  } else if (rk.acc_out) {
     Mv<A, V> a = ldv<V>(rk.acc_in + o);
 #pragma unroll
     for (int i = 0; i < V; i++) a.x[i] = a.x[i] + rk.w * A(t.x[i]);
@@ -179,9 +193,11 @@ __global__ void k_tl_vertex(MeshDev<R> m, int B, Base<R> bs, const R *__restrict
   }
 }
 
-// :274-316, :397-421, thickness tendency :541-561 and the RK update
+// :274-316, :397-421, thickness tendency :541-561 and the RK update.  In FP32 the kernel is held
+// to 48 registers (5 blocks of 256 threads per SM), which measured faster than the 56 it takes
+// otherwise.
 template <typename R, typename A, int V, class NB>
-__global__ void k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_tl_cell(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                           const R *__restrict__ ht, Diag<R> d, RK<R, A> rk, R *tend_h) {
   using M = Mv<R, V>;
   const int nC = m.nC;
@@ -692,9 +708,23 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
   R *tn = is_edge ? out.tu_next : out.th_next;
   const A wn = is_edge ? out.wu : out.wh, cn = is_edge ? out.cu : out.ch;
   Mv<A, V> next;
+  const R *const *pin = is_edge ? out.pad_in_u : out.pad_in_h;
+  R *pout = is_edge ? out.pad_out_u : out.pad_out_h;
   if (out.mode == AD_FINAL) {
     A *dst = is_edge ? out.dst_u : out.dst_h;
-    const Mv<A, V> a = ldv<V>(acc + o), x = ldv<V>(x2 + o);
+    Mv<A, V> a;
+    if (pin[0]) {  // the stored contributions of the three later stages, in stage order
+      a = mv_cast<V, A>(ldv<V>(pin[0] + o));
+#pragma unroll
+      for (int j = 1; j < 3; j++) {
+        const Mv<R, V> pj = ldv<V>(pin[j] + o);
+#pragma unroll
+        for (int i = 0; i < V; i++) a.x[i] = a.x[i] + A(pj.x[i]);
+      }
+    } else {
+      a = ldv<V>(acc + o);
+    }
+    const Mv<A, V> x = ldv<V>(x2 + o);
     Mv<A, V> d;
 #pragma unroll
     for (int i = 0; i < V; i++) {
@@ -703,15 +733,19 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
     }
     stv<V>(dst + o, d);
   } else {
-    Mv<A, V> a;
-    if (out.mode == AD_SET) {
-      a = mv_cast<V, A>(pad);
+    if (pout) {
+      stv<V>(pout + o, pad);
     } else {
-      a = ldv<V>(acc + o);
+      Mv<A, V> a;
+      if (out.mode == AD_SET) {
+        a = mv_cast<V, A>(pad);
+      } else {
+        a = ldv<V>(acc + o);
 #pragma unroll
-      for (int i = 0; i < V; i++) a.x[i] = a.x[i] + A(pad.x[i]);
+        for (int i = 0; i < V; i++) a.x[i] = a.x[i] + A(pad.x[i]);
+      }
+      stv<V>(acc + o, a);
     }
-    stv<V>(acc + o, a);
     if (tn) {
       const Mv<A, V> x = x2 ? ldv<V>(x2 + o) : mv_fill<A, V>(A(0));
 #pragma unroll

@@ -31,6 +31,9 @@ struct MemberBufs {
   R *pu[3] = {}, *ph[3] = {};
   AdWork<R> w{};
   R *pad_u[2] = {}, *pad_h[2] = {};
+  // per-stage tendencies (tangent linear) or contributions (adjoint) of the first three stages
+  // of a step, summed into the FP64 members by its last stage
+  R *tk_u[3] = {}, *tk_h[3] = {};
 };
 
 template <typename R>
@@ -82,6 +85,10 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   for (int k = 0; k < 2; k++) {
     mb->pad_u[k] = walloc<R>(M, Ed, s);
     mb->pad_h[k] = walloc<R>(M, C, s);
+  }
+  for (int k = 0; k < 3; k++) {
+    mb->tk_u[k] = walloc<R>(M, Ed, s);
+    mb->tk_h[k] = walloc<R>(M, C, s);
   }
   M.acc_u = walloc<double>(M, Ed, s);
   M.acc_h = walloc<double>(M, C, s);
@@ -443,9 +450,20 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
       hti = mb->ph[2];
     }
   }
-  double *acu = W.ms[prec].acc_u, *ach = W.ms[prec].acc_h;
-  RK<R, double> rut{du, k == 0 ? du : acu, k == 3 ? du : acu, k < 3 ? mb->pu[k] : nullptr, c[k], w[k], R(0), ph.tc1};
-  RK<R, double> rht{dh, k == 0 ? dh : ach, k == 3 ? dh : ach, k < 3 ? mb->ph[k] : nullptr, c[k], w[k], R(0), 0};
+  // stages 1-3 keep their tendencies; stage 4 sums them into the FP64 members (deferred RK4
+  // accumulation, the same FP64 additions as accumulating stage by stage)
+  RK<R, double> rut{du, nullptr, k == 3 ? du : nullptr, k < 3 ? mb->pu[k] : nullptr, c[k], w[k], R(0), ph.tc1};
+  RK<R, double> rht{dh, nullptr, k == 3 ? dh : nullptr, k < 3 ? mb->ph[k] : nullptr, c[k], w[k], R(0), 0};
+  if (k < 3) {
+    rut.t_out = mb->tk_u[k];
+    rht.t_out = mb->tk_h[k];
+  } else {
+    for (int j = 0; j < 3; j++) {
+      rut.t_in[j] = mb->tk_u[j];
+      rht.t_in[j] = mb->tk_h[j];
+      rut.wt[j] = rht.wt[j] = w[j];
+    }
+  }
   // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
   Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, st);
   Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, st);
@@ -530,6 +548,16 @@ static void ad_member_step(Engine &E, int prec, int B, double *au, double *ah, M
     AdIn<R> in{mb->pad_u[(3 - k) & 1], mb->pad_h[(3 - k) & 1]};
     AdOut<R, double> out{};
     out.acc_u = M.acc_u; out.acc_h = M.acc_h;
+    // stages 4, 3, 2 keep their contributions; stage 1 sums them (deferred accumulation)
+    if (k > 0) {
+      out.pad_out_u = mb->tk_u[3 - k];
+      out.pad_out_h = mb->tk_h[3 - k];
+    } else {
+      for (int j = 0; j < 3; j++) {
+        out.pad_in_u[j] = mb->tk_u[j];
+        out.pad_in_h[j] = mb->tk_h[j];
+      }
+    }
     out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
     out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
     out.tu_next = mb->pad_u[(4 - k) & 1];
@@ -701,13 +729,18 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
   const Base<R> bs = W.st[prec].valid ? stored_base<R>(W, prec, 0, 1) : base_for<R>(W, 1);
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
-  RK<R, double> rku{W.ms[prec].acc_u, W.ms[prec].acc_u, W.ms[prec].acc_u, mb->pu[1], c[1], w[1], R(0), 0};
-  RK<R, double> rkh{W.ms[prec].acc_h, W.ms[prec].acc_h, W.ms[prec].acc_h, mb->ph[1], c[1], w[1], R(0), 0};
+  // a middle stage as the sweeps run it: x0 read, next state and tendency written (deferred
+  // accumulation); the adjoint likewise stores its contribution
+  RK<R, double> rku{W.ms[prec].acc_u, nullptr, nullptr, mb->pu[1], c[1], w[1], R(0), 0};
+  RK<R, double> rkh{W.ms[prec].acc_h, nullptr, nullptr, mb->ph[1], c[1], w[1], R(0), 0};
+  rku.t_out = mb->tk_u[1];
+  rkh.t_out = mb->tk_h[1];
   AdIn<R> in{mb->pad_u[0], mb->pad_h[0]};
   AdOut<R, double> out{};
   out.acc_u = W.ms[prec].acc_u; out.acc_h = W.ms[prec].acc_h; out.mode = AD_ADD;
   out.x2u = W.ms[prec].acc_u; out.x2h = W.ms[prec].acc_h;
   out.tu_next = mb->pad_u[1]; out.th_next = mb->pad_h[1];
+  out.pad_out_u = mb->tk_u[1]; out.pad_out_h = mb->tk_h[1];
   out.wu = w[1]; out.cu = c[1]; out.wh = w[1]; out.ch = c[1];
   auto launch = [&]() {
     using LR = Launch<R, double>;
