@@ -428,6 +428,9 @@ def run_mpsw(a, rank, world):
         out = ctypes.c_double()
         eng.h.check(L.mpsw_time_kernel(eng.h.ptr, i, FP32, B, 20, ctypes.byref(out)), 'time_kernel')
         kt[name] = out.value
+    vb = (ctypes.c_int * 16)()
+    eng.h.check(L.mpsw_window_tuning(eng.h.ptr, FP32, B, vb), 'window_tuning')
+    tuning = {k: {'v': vb[2 * i], 'block': vb[2 * i + 1]} for i, k in enumerate(KERNELS[:8])}
     # every member kernel launches once per stage: the dominant one is the slowest
     top = max(KERNELS[:8], key=lambda k: kt[k])
     bytes_ = kernel_bytes(top, nC, nE, nV, sum_eoe, B, 4)
@@ -438,7 +441,7 @@ def run_mpsw(a, rank, world):
     roof = {'bound': 'hbm', 'kernel': top, 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
             'frac': ach / hbm, 'peak_source': peak_kind, 'traffic': traffic_of(top, a.level, B),
             'algorithmic_bytes': bytes_, 'ms_per_launch': kt[top],
-            'kernel_ms': {k: kt[k] for k in KERNELS[:8]}, 'stages': stages}
+            'kernel_ms': {k: kt[k] for k in KERNELS[:8]}, 'stages': stages, 'tuning': tuning}
 
     # host baseline: serial oracle on one core, bounded sample
     cpu = None

@@ -115,6 +115,13 @@ int mpsw_window_init(mpsw_handle *h, int nsteps, int ckpt_every, void *stream);
  * (checkpoints only); mode 1, 2, 3: FP64, FP32, both, regardless of size.  A stage slot holds
  * 6 nEdges + 2 nVertices + nCells values, nsteps * 4 slots per stored precision. */
 int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes);
+/* Launch choices of the eight member kernels (tl_vertex, tl_cell, tl_edge_diag, tl_edge_tend,
+ * ad_edge, ad_cell, ad_vertex, ad_final) picked for (precision, B): v_block[2k] members per
+ * thread, v_block[2k+1] threads per block; zeros when not tuned.  No counterpart in the
+ * reference.  The first sweep of a window for a given (precision, B) times each kernel over the
+ * pairs B allows on the window's own buffers and keeps the fastest (MPSW_TUNE=0 in the
+ * environment keeps fixed defaults). */
+int mpsw_window_tuning(mpsw_handle *h, int precision, int B, int *v_block);
 /* Tangent linear over the window, B members in place: du [nEdges][B], dh [nCells][B]. */
 int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh, void *stream);
 /* Adjoint over the window, B members in place: on entry the adjoint of the final state, on

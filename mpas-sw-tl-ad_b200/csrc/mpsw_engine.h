@@ -74,6 +74,8 @@ struct Window {
     // captured graphs do not depend on where the caller keeps its members
     double *x_u = nullptr, *x_h = nullptr;
   } ms[2];
+  // autotuned launch choices of the member kernels, per precision and member count
+  std::map<int, TuneTable> tune[2];
 };
 
 // A captured CUDA graph of one window step, keyed by what its kernels bake in.
@@ -208,6 +210,8 @@ struct Engine {
   void window_ad(int prec, int B, double *au, double *ah, cudaStream_t s);
   void window_final(double *u, double *h, cudaStream_t s);
   double time_kernel(int which, int prec, int B, int iters);
+  const TuneTable *tuning(int prec, int B);
+  const TuneTable *tuned_for(int prec, int B);
   void state_from_device(const double *u, const double *h, cudaStream_t s);
   void state_to_device(double *u, double *h, cudaStream_t s);
   void to_internal(int kind, int B, const double *src, double *dst, cudaStream_t s);

@@ -5,6 +5,7 @@
 namespace mpsw {
 
 long long g_launches = 0;
+thread_local const TuneTable *g_tune = nullptr;
 
 int grid_for(long long total) {
   long long g = (total + kThreads - 1) / kThreads;

@@ -13,19 +13,29 @@
 
 namespace mpsw {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 
-// Grid and block for `total` threads: 256-thread blocks, halved (down to 64) while that leaves
-// fewer than two blocks per SM, so thin single-trajectory launches still spread over all SMs.
+// Grid and block for `total` threads: 128-thread blocks (measured faster than 256 for the
+// latency-bound gathers here), halved (down to 64) while that leaves fewer than two blocks per
+// SM, so thin single-trajectory launches still spread over all SMs.
 struct LaunchCfg {
   int grid, block;
   size_t smem = 0;  // dynamic shared memory bytes
 };
-inline LaunchCfg launch_cfg(long long total) {
-  int block = kThreads;
+// MPSW_BLOCK=64|128|256 overrides the starting block size.
+inline int block_threads() {
+  static const int b = [] {
+    const char *e = std::getenv("MPSW_BLOCK");
+    const int v = e ? std::atoi(e) : 0;
+    return (v == 64 || v == 128 || v == 256) ? v : kThreads;
+  }();
+  return b;
+}
+inline LaunchCfg launch_cfg(long long total, int block0 = 0) {
+  int block = block0 ? block0 : block_threads();
   while (block > 64 && total < 2LL * 148 * block) block >>= 1;
   long long g = (total + block - 1) / block;
-  const long long cap = 148LL * 16 * (kThreads / block);
+  const long long cap = 148LL * 32 * 128 / block;  // grid-stride beyond 4096 threads per SM
   if (g < 1) g = 1;
   return {(int)(g < cap ? g : cap), block, 0};
 }
@@ -91,13 +101,17 @@ inline bool stage_enabled() {
 }
 // (and the block's stage fits the default 48 KB of dynamic shared memory)
 template <typename R>
-inline bool use_staged(const MeshDev<R> &m, int B, int v, size_t smem_per_edge_bytes) {
-  const int tpe = B / v;
+inline bool use_staged(const MeshDev<R> &m, int B, int v, size_t smem_per_edge_bytes, int block0 = 0) {
+  const int tpe = B / v, bt = block0 ? block0 : block_threads();
   return stage_enabled() && m.max_eoe <= BoundsNarrow::e2 && m.max_eoc <= BoundsNarrow::c && tpe <= 128 &&
-         smem_per_edge_bytes * (kThreads / tpe) <= 48 * 1024;
+         tpe <= bt / 2 && smem_per_edge_bytes * (bt / tpe) <= 48 * 1024;
 }
-inline LaunchCfg staged_cfg(int n, int B, int v, size_t smem_per_edge_bytes) {
-  const int tpe = B / v, epb = kThreads / tpe;
+
+// the autotuned members-per-thread and block of a member kernel (0: default)
+inline int tuned_v(KernelId k) { return g_tune ? g_tune->k[k].v : 0; }
+inline int tuned_block(KernelId k) { return g_tune ? g_tune->k[k].block : 0; }
+inline LaunchCfg staged_cfg(int n, int B, int v, size_t smem_per_edge_bytes, int block0 = 0) {
+  const int tpe = B / v, epb = (block0 ? block0 : block_threads()) / tpe;
   return {(n + epb - 1) / epb, epb * tpe, smem_per_edge_bytes * epb};
 }
 
@@ -172,16 +186,19 @@ template <typename R, typename A>
 void Launch<R, A>::tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                              const Diag<R> &d, cudaStream_t s) {
   g_launches++;
-  const int v = vec_width<R, A>(B, {ut, ht, d.circ, d.vort, d.hv, d.pvv});
-  MPSW_VDISPATCH(v, (launch_k(k_tl_vertex<R, VV>, launch_cfg((long long)(m.nV) * ((B) / (VV))), s, m, B, bs, ut, ht, d)));
+  const int v = vec_width<R, A>(B, {ut, ht, d.circ, d.vort, d.hv, d.pvv}, tuned_v(K_TL_VERTEX));
+  const int bk = tuned_block(K_TL_VERTEX);
+  MPSW_VDISPATCH(v, (launch_k(k_tl_vertex<R, VV>, launch_cfg((long long)(m.nV) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, d)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                            const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.div, d.ke, d.pc, d.vc, d.pvv, d.vort, tend_h, rk.x0, rk.acc_in,
-                                    rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1], rk.t_in[2]});
-  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_cell<R, A, VV, NB>, launch_cfg((long long)(m.nC) * ((B) / (VV))), s, m, B, bs, ut, ht, d, rk, tend_h)));
+                                    rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1], rk.t_in[2]},
+                                tuned_v(K_TL_CELL));
+  const int bk = tuned_block(K_TL_CELL);
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_cell<R, A, VV, NB>, launch_cfg((long long)(m.nC) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, d, rk, tend_h)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
@@ -190,8 +207,9 @@ void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, c
   Diag<R> dd = d;
   if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
   const int v = vec_width<R, A>(B, {ut, ht, dd.pvv, dd.pc, dd.div, dd.vort, dd.pe, dd.he, dd.v, dd.gpt, dd.gpn, dd.dsq_u},
-                                kWideV<R>);
-  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, dd, ph)));
+                                tuned_v(K_TL_EDGE_DIAG) ? tuned_v(K_TL_EDGE_DIAG) : kWideV<R>);
+  const int bk = tuned_block(K_TL_EDGE_DIAG);
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, dd, ph)));
 }
 template <typename R, typename A>
 void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
@@ -200,14 +218,16 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
                                     rk.x0, rk.acc_in, rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1],
-                                    rk.t_in[2]});
+                                    rk.t_in[2]},
+                                tuned_v(K_TL_EDGE_TEND));
+  const int bk = tuned_block(K_TL_EDGE_TEND);
   constexpr int J = BoundsNarrow::e2;
-  if (use_staged(m, B, v, eoe_stage_bytes<R, J, 3>(1))) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eoe_stage_bytes<R, J, 3>(1)),
+  if (use_staged(m, B, v, eoe_stage_bytes<R, J, 3>(1), bk)) {
+    MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eoe_stage_bytes<R, J, 3>(1), bk),
                                s, m, B, bs, ut, ht, d, ph, rk, tend_u));
     return;
   }
-  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_tend<R, A, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV))), s, m, B, bs, ut, ht, d, ph, rk, tend_u)));
+  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_tend<R, A, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, d, ph, rk, tend_u)));
 }
 // members per thread of one adjoint stage: every buffer the five kernels touch
 template <typename R, typename A>
@@ -220,16 +240,25 @@ static int ad_width(int B, const AdIn<R> &in, const AdWork<R> &w, const AdOut<R,
                          prefer);
 }
 
+// preferred members per thread of adjoint kernel `which` (0 edge, 1 cell, 2 vertex, 3 final,
+// 4-5 del4): the autotuned width, else 8 for ad_final in FP32, else the default
+template <typename R>
+inline int ad_prefer(int which) {
+  static const KernelId ids[4] = {K_AD_EDGE, K_AD_CELL, K_AD_VERTEX, K_AD_FINAL};
+  if (which < 4 && tuned_v(ids[which])) return tuned_v(ids[which]);
+  return which == 3 ? kWideV<R> : 0;
+}
+
 template <typename R, typename A, int V, class NB>
 static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                       const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w, const AdOut<R, A> &out,
                       cudaStream_t s) {
   g_launches++;
   switch (which) {
-    case 0: launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
-    case 1: launch_k(k_ad_cell<R, A, V, NB>, launch_cfg((long long)(m.nC) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
-    case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V))), s, m, B, bs, ph, in, sd, w); break;
-    case 3: launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V))), s, m, B, bs, w, out); break;
+    case 0: launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V)), tuned_block(K_AD_EDGE)), s, m, B, bs, ph, in, sd, w); break;
+    case 1: launch_k(k_ad_cell<R, A, V, NB>, launch_cfg((long long)(m.nC) * ((B) / (V)), tuned_block(K_AD_CELL)), s, m, B, bs, ph, in, sd, w); break;
+    case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V)), tuned_block(K_AD_VERTEX)), s, m, B, bs, ph, in, sd, w); break;
+    case 3: launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), tuned_block(K_AD_FINAL)), s, m, B, bs, w, out); break;
     case 4: launch_k(k_ad_del4_vc<R, V, NB>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (V))), s, m, B, ph, in, w); break;
     default: launch_k(k_ad_del4_e<R, V>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, w); break;
   }
@@ -239,27 +268,27 @@ template <typename R, typename A>
 void Launch<R, A>::ad_stage(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                             const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w,
                             const AdOut<R, A> &out, cudaStream_t s) {
-  const int v = ad_width<R, A>(B, in, w, out);
-  MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, {
-    ad_launch<R, A, VV, NB>(0, m, B, bs, ph, in, sd, w, out, s);
-    if (ph.visc4 > R(0)) {
-      ad_launch<R, A, VV, NB>(4, m, B, bs, ph, in, sd, w, out, s);
-      ad_launch<R, A, VV, NB>(5, m, B, bs, ph, in, sd, w, out, s);
-    }
-    ad_launch<R, A, VV, NB>(1, m, B, bs, ph, in, sd, w, out, s);
-    ad_launch<R, A, VV, NB>(2, m, B, bs, ph, in, sd, w, out, s);
-  }));
-  const int vf = ad_width<R, A>(B, in, w, out, kWideV<R>);  // ad_final runs wider
-  MPSW_VDISPATCH(vf, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(3, m, B, bs, ph, in, sd, w, out, s)));
+  // each kernel at its own width (autotuned, else the default; ad_final defaults wider)
+  auto one = [&](int which) {
+    const int vk = ad_width<R, A>(B, in, w, out, ad_prefer<R>(which));
+    MPSW_VDISPATCH(vk, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(which, m, B, bs, ph, in, sd, w, out, s)));
+  };
+  one(0);
+  if (ph.visc4 > R(0)) {
+    one(4);
+    one(5);
+  }
+  one(1);
+  one(2);
+  one(3);
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                            const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out,
                            cudaStream_t s) {
   const AdSeeds<R> sd{};
-  const int v = ad_width<R, A>(B, in, w, out);
   const int k = which < 0 || which > 3 ? 3 : which;
-  const int vk = k == 3 ? ad_width<R, A>(B, in, w, out, kWideV<R>) : v;
+  const int vk = ad_width<R, A>(B, in, w, out, ad_prefer<R>(k));
   MPSW_VDISPATCH(vk, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(k, m, B, bs, ph, in, sd, w, out, s)));
 }
 template <typename R, typename A>

@@ -12,6 +12,27 @@ namespace mpsw {
 int grid_for(long long total);
 extern long long g_launches;
 
+// Launch choices of the member kernels, picked per (precision, B) by the window's autotuner:
+// members per thread and threads per block (0: the default choice).
+enum KernelId {
+  K_TL_VERTEX, K_TL_CELL, K_TL_EDGE_DIAG, K_TL_EDGE_TEND, K_AD_EDGE, K_AD_CELL, K_AD_VERTEX, K_AD_FINAL,
+  K_TUNED
+};
+struct TuneCfg {
+  int v = 0, block = 0;
+};
+struct TuneTable {
+  TuneCfg k[K_TUNED];
+};
+// The table the launchers of the calling thread follow (null: defaults); set for the duration
+// of a sweep by TuneScope.
+extern thread_local const TuneTable *g_tune;
+struct TuneScope {
+  const TuneTable *prev;
+  explicit TuneScope(const TuneTable *t) : prev(g_tune) { g_tune = t; }
+  ~TuneScope() { g_tune = prev; }
+};
+
 template <typename R, typename A>
 struct Launch {
   // forward stage pieces (single trajectory)

@@ -62,6 +62,7 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   if (M.bufs && M.B >= B) return (MemberBufs<R> *)M.bufs;
   E.graphs_free();  // captured steps point at the buffers about to be replaced
   free_members<R>(M);
+  E.win.tune[prec].clear();
   auto *mb = new MemberBufs<R>();
   const size_t C = (size_t)E.nC * B, Ed = (size_t)E.nE * B, V = (size_t)E.nV * B;
   Diag<R> &d = mb->d;
@@ -649,10 +650,11 @@ void Engine::window_tl(int prec, int B, double *du, double *dh, cudaStream_t s) 
   if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
   if (B < 1 || !du || !dh) throw EngineError(MPSW_ERR_ARG, "window_tl needs B >= 1 and member buffers");
   if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
+  if (prec != 0 && prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   join(s, stream, true);
+  TuneScope scope(tuning(prec, B));
   if (prec == 0) window_tl_impl<double>(*this, prec, B, du, dh);
-  else if (prec == 1) window_tl_impl<float>(*this, prec, B, du, dh);
-  else throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+  else window_tl_impl<float>(*this, prec, B, du, dh);
   join(s, stream, false);
 }
 
@@ -660,11 +662,12 @@ void Engine::window_ad(int prec, int B, double *au, double *ah, cudaStream_t s) 
   if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
   if (B < 1 || !au || !ah) throw EngineError(MPSW_ERR_ARG, "window_ad needs B >= 1 and member buffers");
   if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
+  if (prec != 0 && prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   join(s, stream, true);
   window_ensure();
+  TuneScope scope(tuning(prec, B));
   if (prec == 0) window_ad_impl<double>(*this, prec, B, au, ah);
-  else if (prec == 1) window_ad_impl<float>(*this, prec, B, au, ah);
-  else throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+  else window_ad_impl<float>(*this, prec, B, au, ah);
   join(s, stream, false);
 }
 
@@ -784,8 +787,55 @@ double Engine::time_kernel(int which, int prec, int B, int iters) {
   if (!win.nsteps) throw EngineError(MPSW_ERR_STATE, "mpsw_window_init has not been called");
   if (which < 0 || which > 9 || B < 1 || iters < 1) throw EngineError(MPSW_ERR_ARG, "bad kernel timing request");
   window_ensure();
+  TuneScope scope(tuned_for(prec, B));  // the launch choices the sweeps use
   return prec == 1 ? time_kernel_impl<float>(*this, which, prec, B, iters)
                    : time_kernel_impl<double>(*this, which, prec, B, iters);
+}
+
+// Autotuner of the member kernels: for each of the eight tangent-linear / adjoint kernels, time
+// every (members per thread, threads per block) pair the member count allows on the window's own
+// buffers (mpsw_time_kernel's launch of a middle stage) and keep the fastest.  Runs once per
+// (precision, B) before the first sweep captures its graphs, so the graphs bake in the choice;
+// MPSW_TUNE=0 keeps the default choices.
+template <typename R>
+static TuneTable tune_members(Engine &E, int prec, int B) {
+  TuneTable best{};
+  const int vs[] = {1, 2, 4, 8}, blocks[] = {64, 128, 256};
+  for (int k = 0; k < K_TUNED; k++) {
+    double tbest = 1e30;
+    for (int v : vs) {
+      if (B % v || (sizeof(R) == 8 && v > 4) || (sizeof(R) == 4 && v < 2 && B % 2 == 0)) continue;
+      for (int bl : blocks) {
+        TuneTable trial = best;
+        trial.k[k].v = v;
+        trial.k[k].block = bl;
+        TuneScope scope(&trial);
+        const double t = time_kernel_impl<R>(E, k, prec, B, 4);
+        if (t < tbest) {
+          tbest = t;
+          best.k[k] = trial.k[k];
+        }
+      }
+    }
+  }
+  return best;
+}
+
+// The table for (prec, B), tuning it first when needed (before any graph of it is captured).
+const TuneTable *Engine::tuning(int prec, int B) {
+  static const bool enabled = !(getenv("MPSW_TUNE") && atoi(getenv("MPSW_TUNE")) == 0);
+  if (!enabled) return nullptr;
+  auto it = win.tune[prec].find(B);
+  if (it != win.tune[prec].end()) return &it->second;
+  const TuneTable t = prec == 1 ? tune_members<float>(*this, prec, B) : tune_members<double>(*this, prec, B);
+  graphs_free();  // nothing captured before this point may keep the untuned choices
+  return &(win.tune[prec][B] = t);
+}
+
+// The table for (prec, B) if it has been tuned, else null (defaults).
+const TuneTable *Engine::tuned_for(int prec, int B) {
+  auto it = win.tune[prec].find(B);
+  return it == win.tune[prec].end() ? nullptr : &it->second;
 }
 
 }  // namespace mpsw
@@ -797,6 +847,17 @@ int mpsw_to_internal(mpsw_handle *h, int kind, int B, const double *src, double 
 }
 int mpsw_to_reference(mpsw_handle *h, int kind, int B, const double *src, double *dst, void *stream) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.to_reference(kind, B, src, dst, (cudaStream_t)stream); });
+}
+int mpsw_window_tuning(mpsw_handle *h, int precision, int B, int *v_block) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) {
+    if (!v_block) throw mpsw::EngineError(MPSW_ERR_ARG, "null output");
+    if (precision != 0 && precision != 1) throw mpsw::EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+    const mpsw::TuneTable *t = e.tuned_for(precision, B);
+    for (int k = 0; k < mpsw::K_TUNED; k++) {
+      v_block[2 * k] = t ? t->k[k].v : 0;
+      v_block[2 * k + 1] = t ? t->k[k].block : 0;
+    }
+  });
 }
 int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_storage(mode, max_bytes); });
