@@ -130,6 +130,18 @@ int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah,
 /* Final nonlinear state of the window (device buffers, internal order). */
 int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream);
 
+/* ---- initial conditions ------------------------------------------------------------------
+ * Box average of a regular latitude-longitude field onto points, as the reference's grid2mpas
+ * (src/grid2mpas.f90:21-70) does for its ERA5 initialisation: for each point (lat[k], lon[k], in
+ * the units of the axes) the nearest axis entries (first minimum of the distance) and the mean
+ * of the up to 3 x 3 grid values around them, clamped at the axis ends.  grid is [nlat][nlon]
+ * (row-major, latitude rows), lat1d / lon1d the axes; all device buffers.  The reference shifts
+ * negative longitudes of its arguments into latitudes by mistake (:46-47); callers here shift
+ * longitudes into [0, 360) before the call (mpsw/ic.py: era_to_mpas). */
+int mpsw_grid_to_points(mpsw_handle *h, int nlat, int nlon, const double *lat1d, const double *lon1d,
+                        const double *grid, long long n, const double *lat, const double *lon, double *out,
+                        void *stream);
+
 /* ---- tendencies without device allocation ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory when they
  * need the model (a host system that reserves all GPU memory for its own pool at start-up, or

@@ -31,6 +31,7 @@ UNITS = [
     ('mpsw_engine.cu', ['--fmad=false']),
     ('mpsw_window.cu', ['--fmad=false']),
     ('mpsw_noalloc.cu', ['--fmad=false']),
+    ('mpsw_ic.cu', ['--fmad=false']),
     ('mpsw_setup.cpp', ['--fmad=false', '-x', 'cu']),
 ]
 HEADERS = ['mpsw_internal.h', 'mpsw_kernels.cuh', 'mpsw_launch.h', 'mpsw_launch.cuh', 'mpsw_members.cuh',

@@ -45,6 +45,7 @@ SIGNATURES = {
     'mpsw_to_internal': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     'mpsw_to_reference': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     'mpsw_forward': (_c_int, [_vp, _c_int, _c_int]),
+    'mpsw_grid_to_points': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _vp]),
     'mpsw_get_stream': (_c_int, [_vp, ctypes.POINTER(_vp)]),
     'mpsw_window_init': (_c_int, [_vp, _c_int, _c_int, _vp]),
     'mpsw_window_storage': (_c_int, [_vp, _c_int, ctypes.c_double]),

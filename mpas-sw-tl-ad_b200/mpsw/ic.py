@@ -164,3 +164,70 @@ def workload(level: int, seed: int = 0, topography: bool = False):
         st['h'] = st['h'] - h_s
     st['h_s'] = h_s
     return unit, mesh, st
+
+
+# ---- real-data initialisation (the reference driver's test case 7) ------------------------------
+def era_to_mpas(lat_grid, lon_grid, var_grid, lat, lon, handle=None):
+    """A regular latitude-longitude field (degrees; 1-D axes or the 2-D meshgrid of them) averaged
+    onto points (degrees) by the GPU box average of ``mpsw_grid_to_points``, as the reference's
+    era2mpas / grid2mpas (src/mpas_sw_driver.py:147-158, src/grid2mpas.f90:21-70): longitudes
+    are taken into [0, 360) for the points and the grid (the reference shifts them into the
+    latitudes instead, a slip fixed here), and points whose average is NaN get the mean of the
+    others.  Returns a float64 numpy array."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+    lat_grid, lon_grid = np.asarray(lat_grid, dtype=np.float64), np.asarray(lon_grid, dtype=np.float64)
+    lat1d = lat_grid[:, 0] if lat_grid.ndim == 2 else lat_grid
+    lon1d = lon_grid[0, :] if lon_grid.ndim == 2 else lon_grid
+    lon1d = np.where(lon1d < 0, lon1d + 360.0, lon1d)
+    pts_lon = np.asarray(lon, dtype=np.float64).ravel().copy()
+    pts_lon[pts_lon < 0] += 360.0
+    pts_lat = np.asarray(lat, dtype=np.float64).ravel()
+    grid = np.ascontiguousarray(var_grid, dtype=np.float64)
+    if grid.shape != (lat1d.size, lon1d.size):
+        raise ValueError('field shape %s does not match the axes (%d, %d)' % (grid.shape, lat1d.size, lon1d.size))
+    own = handle is None
+    h = _lib.Handle() if own else handle
+    try:
+        dev = [torch.tensor(np.ascontiguousarray(x), device='cuda') for x in (lat1d, lon1d, grid, pts_lat, pts_lon)]
+        out = torch.empty(pts_lat.size, dtype=torch.float64, device='cuda')
+        p = [ctypes.c_void_p(x.data_ptr()) for x in dev]
+        h.call('mpsw_grid_to_points', lat1d.size, lon1d.size, p[0], p[1], p[2], pts_lat.size, p[3], p[4],
+               ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        var = out.cpu().numpy()
+    finally:
+        if own:
+            h.close()
+    bad = np.isnan(var)
+    if bad.any():
+        var[bad] = var[~bad].mean()
+    return var
+
+
+def init_real(module, lat_grid, lon_grid, z_grid, u_grid, v_grid):
+    """The reference driver's real-data initial condition (mpsw_init_real, src/mpas_sw_driver.py:
+    161-216) on a module loaded with a unit-sphere grid: mesh scaled to the Earth's radius,
+    Coriolis parameters, h from the geopotential z / g and the normal wind from the zonal and
+    meridional winds rotated by angleEdge, each averaged onto the mesh by ``era_to_mpas``.
+    The fields are one time of the reanalysis, (nlat, nlon) in degrees."""
+    a = A_EARTH
+    for k in ('xcell', 'ycell', 'zcell', 'xvertex', 'yvertex', 'zvertex', 'xedge', 'yedge', 'zedge',
+              'dvedge', 'dcedge'):
+        setattr(module, k, np.asarray(getattr(module, k)) * a)
+    for k in ('areacell', 'areatriangle', 'kiteareasonvertex'):
+        setattr(module, k, np.asarray(getattr(module, k)) * a ** 2.0)
+    alpha = 0.0
+    late, lone = np.asarray(module.latedge), np.asarray(module.lonedge)
+    latv, lonv = np.asarray(module.latvertex), np.asarray(module.lonvertex)
+    module.fedge = 2.0 * OMEGA * (-np.cos(lone) * np.cos(late) * np.sin(alpha) + np.sin(late) * np.cos(alpha))
+    module.fvertex = 2.0 * OMEGA * (-np.cos(lonv) * np.cos(latv) * np.sin(alpha) + np.sin(latv) * np.cos(alpha))
+    r2d = 180.0 / np.pi
+    latc, lonc = np.asarray(module.latcell).ravel() * r2d, np.asarray(module.loncell).ravel() * r2d
+    module.h[0, 0] = era_to_mpas(lat_grid, lon_grid, np.asarray(z_grid) / GRAVITY, latc, lonc)
+    ue = era_to_mpas(lat_grid, lon_grid, u_grid, late.ravel() * r2d, lone.ravel() * r2d)
+    ve = era_to_mpas(lat_grid, lon_grid, v_grid, late.ravel() * r2d, lone.ravel() * r2d)
+    ang = np.asarray(module.angleedge).ravel()
+    module.u[0, 0] = np.cos(ang) * ue + np.sin(ang) * ve

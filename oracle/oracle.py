@@ -300,3 +300,26 @@ def load_mesh(mod, mesh: dict, ntracers: int = 1):
               'cellsOnCell', 'verticesOnCell', 'verticesOnEdge', 'edgesOnVertex', 'cellsOnVertex',
               'kiteAreasOnVertex', 'meshDensity'):
         setattr(mod, k.lower(), np.asarray(mesh[k]).T)
+
+
+def grid_to_points(lat1d, lon1d, grid, lat, lon):
+    """Restatement of grid2mpas (src/grid2mpas.f90:21-70) for points whose longitudes are already
+    in the axis range: for each point the first index of the minimum |axis - x| in latitude and
+    in longitude (minloc, :53-63), the section of up to 3 x 3 values around them clamped at the
+    axis ends, summed in Fortran element order (latitude fastest, :65-66) and divided by its
+    size.  Loops over points in Python: small cases only."""
+    lat1d, lon1d = np.asarray(lat1d, dtype=np.float64), np.asarray(lon1d, dtype=np.float64)
+    grid = np.asarray(grid, dtype=np.float64)
+    nlat, nlon = lat1d.size, lon1d.size
+    out = np.empty(len(lat))
+    for k, (y, x) in enumerate(zip(np.asarray(lat, dtype=np.float64), np.asarray(lon, dtype=np.float64))):
+        i0 = int(np.argmin(np.abs(y - lat1d)))
+        j0 = int(np.argmin(np.abs(x - lon1d)))
+        i1, i2 = max(i0 - 1, 0), min(i0 + 1, nlat - 1)
+        j1, j2 = max(j0 - 1, 0), min(j0 + 1, nlon - 1)
+        s = 0.0
+        for j in range(j1, j2 + 1):
+            for i in range(i1, i2 + 1):
+                s = s + float(grid[i, j])
+        out[k] = s / float((i2 - i1 + 1) * (j2 - j1 + 1))
+    return out
