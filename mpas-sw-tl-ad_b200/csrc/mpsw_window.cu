@@ -794,7 +794,8 @@ double Engine::time_kernel(int which, int prec, int B, int iters) {
 
 // Autotuner of the member kernels: for each of the eight tangent-linear / adjoint kernels, time
 // every (members per thread, threads per block) pair the member count allows on the window's own
-// buffers (mpsw_time_kernel's launch of a middle stage) and keep the fastest.  Runs once per
+// buffers (mpsw_time_kernel's launch of a middle stage; the better of two 8-launch averages) and
+// keep the fastest.  Runs once per
 // (precision, B) before the first sweep captures its graphs, so the graphs bake in the choice;
 // MPSW_TUNE=0 keeps the default choices.
 template <typename R>
@@ -810,7 +811,7 @@ static TuneTable tune_members(Engine &E, int prec, int B) {
         trial.k[k].v = v;
         trial.k[k].block = bl;
         TuneScope scope(&trial);
-        const double t = time_kernel_impl<R>(E, k, prec, B, 4);
+        const double t = std::min(time_kernel_impl<R>(E, k, prec, B, 8), time_kernel_impl<R>(E, k, prec, B, 8));
         if (t < tbest) {
           tbest = t;
           best.k[k] = trial.k[k];
