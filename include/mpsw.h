@@ -120,7 +120,8 @@ int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes);
  * thread, v_block[2k+1] threads per block; zeros when not tuned.  No counterpart in the
  * reference.  The first sweep of a window for a given (precision, B) times each kernel over the
  * pairs B allows on the window's own buffers and keeps the fastest (MPSW_TUNE=0 in the
- * environment keeps fixed defaults). */
+ * environment keeps fixed defaults; MPSW_TUNE_CACHE=<file> keeps the choices in a text file
+ * keyed by device, mesh size, precision and B, and reuses them). */
 int mpsw_window_tuning(mpsw_handle *h, int precision, int B, int *v_block);
 /* Tangent linear over the window, B members in place: du [nEdges][B], dh [nCells][B]. */
 int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh, void *stream);

@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <string>
 #include <cstring>
 
 #include "mpsw.h"
@@ -62,7 +64,6 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   if (M.bufs && M.B >= B) return (MemberBufs<R> *)M.bufs;
   E.graphs_free();  // captured steps point at the buffers about to be replaced
   free_members<R>(M);
-  E.win.tune[prec].clear();
   auto *mb = new MemberBufs<R>();
   const size_t C = (size_t)E.nC * B, Ed = (size_t)E.nE * B, V = (size_t)E.nV * B;
   Diag<R> &d = mb->d;
@@ -822,13 +823,65 @@ static TuneTable tune_members(Engine &E, int prec, int B) {
   return best;
 }
 
+// Tuning results can be kept in a text file (MPSW_TUNE_CACHE=path), one line per key:
+// "<device name>|<nCells>|<nEdges>|<nVertices>|<precision>|<B>" then 8 pairs "v block".  A
+// process finding its key there skips the timing (so, for example, a profiled run uses the
+// choices of an unprofiled one).
+static std::string tune_key(const Engine &E, int prec, int B) {
+  int dev = 0;
+  cudaDeviceProp p{};
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&p, dev) != cudaSuccess) p.name[0] = 0;
+  std::string name(p.name);
+  for (char &c : name)
+    if (c == ' ' || c == '|') c = '_';
+  return name + "|" + std::to_string(E.nC) + "|" + std::to_string(E.nE) + "|" + std::to_string(E.nV) + "|" +
+         std::to_string(prec) + "|" + std::to_string(B);
+}
+
+static bool tune_cache_read(const std::string &path, const std::string &key, TuneTable *t) {
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return false;
+  char line[1024];
+  bool found = false;
+  while (fgets(line, sizeof line, f)) {
+    char k[512];
+    int v[2 * K_TUNED];
+    if (sscanf(line, "%511s %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d", k, &v[0], &v[1], &v[2], &v[3], &v[4],
+               &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11], &v[12], &v[13], &v[14], &v[15]) != 17 ||
+        key != k)
+      continue;
+    for (int i = 0; i < K_TUNED; i++) {
+      t->k[i].v = v[2 * i];
+      t->k[i].block = v[2 * i + 1];
+    }
+    found = true;  // the last line for a key wins
+  }
+  fclose(f);
+  return found;
+}
+
+static void tune_cache_append(const std::string &path, const std::string &key, const TuneTable &t) {
+  FILE *f = fopen(path.c_str(), "a");
+  if (!f) return;  // a cache that cannot be written only costs a re-tune
+  fprintf(f, "%s", key.c_str());
+  for (int i = 0; i < K_TUNED; i++) fprintf(f, " %d %d", t.k[i].v, t.k[i].block);
+  fprintf(f, "\n");
+  fclose(f);
+}
+
 // The table for (prec, B), tuning it first when needed (before any graph of it is captured).
 const TuneTable *Engine::tuning(int prec, int B) {
   static const bool enabled = !(getenv("MPSW_TUNE") && atoi(getenv("MPSW_TUNE")) == 0);
   if (!enabled) return nullptr;
   auto it = win.tune[prec].find(B);
   if (it != win.tune[prec].end()) return &it->second;
-  const TuneTable t = prec == 1 ? tune_members<float>(*this, prec, B) : tune_members<double>(*this, prec, B);
+  const char *cache = getenv("MPSW_TUNE_CACHE");
+  const std::string key = tune_key(*this, prec, B);
+  TuneTable t{};
+  if (!(cache && *cache && tune_cache_read(cache, key, &t))) {
+    t = prec == 1 ? tune_members<float>(*this, prec, B) : tune_members<double>(*this, prec, B);
+    if (cache && *cache) tune_cache_append(cache, key, t);
+  }
   graphs_free();  // nothing captured before this point may keep the untuned choices
   return &(win.tune[prec][B] = t);
 }

@@ -144,3 +144,31 @@ def test_member_width_does_not_change_results(precision):
                 assert torch.equal(x[:, 0], y[:, b])
             else:  # FP32 stencils are compiled with contraction: allow one rounding per op
                 assert rel(x[:, 0].cpu().numpy(), y[:, b].cpu().numpy()) < 1e-6
+
+
+def test_tuning_cache_file(tmp_path, monkeypatch):
+    """The autotuner writes its choice for (mesh, precision, B) to MPSW_TUNE_CACHE, and an engine
+    finding the key there takes it from the file."""
+    import ctypes
+    from mpsw import _lib
+    cache = tmp_path / 'tune.txt'
+    monkeypatch.setenv('MPSW_TUNE_CACHE', str(cache))
+    m, e = engine(level=2)
+    du, dh = members(m, 8, 11)
+    w = e.window(2, ckpt_every=1)
+    w.tl(du, dh, 1)
+    lines = cache.read_text().split('\n')
+    key_lines = [l for l in lines if l.strip()]
+    assert len(key_lines) == 1 and key_lines[0].split()[0].endswith('|1|8')
+    # a different choice under the same key in the file is taken by a new engine
+    vals = [8, 64] * 8
+    cache.write_text(key_lines[0].split()[0] + ' ' + ' '.join(map(str, vals)) + '\n')
+    m2, e2 = engine(level=2)
+    w2 = e2.window(2, ckpt_every=1)
+    a = w2.tl(du, dh, 1)
+    out = (ctypes.c_int * 16)()
+    e2.h.check(_lib.load().mpsw_window_tuning(e2.h.ptr, 1, 8, out), 'tuning')
+    assert list(out) == vals
+    b = w.tl(du, dh, 1)
+    for x, y in zip(a, b):  # FP32 stencils: the launch choice may move a rounding, no more
+        assert rel(x.cpu().numpy(), y.cpu().numpy()) < 1e-6
