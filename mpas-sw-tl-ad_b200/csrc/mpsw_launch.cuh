@@ -209,6 +209,12 @@ void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, c
   const int v = vec_width<R, A>(B, {ut, ht, dd.pvv, dd.pc, dd.div, dd.vort, dd.pe, dd.he, dd.v, dd.gpt, dd.gpn, dd.dsq_u},
                                 tuned_v(K_TL_EDGE_DIAG) ? tuned_v(K_TL_EDGE_DIAG) : kWideV<R>);
   const int bk = tuned_block(K_TL_EDGE_DIAG);
+  constexpr int J = BoundsNarrow::e2;
+  constexpr size_t eb = eoe_stage_bytes<R, J, 1, 0>();
+  if (use_staged(m, B, v, eb, bk)) {
+    MPSW_VDISPATCH(v, launch_k(k_tl_edge_diag_st<R, VV, J>, staged_cfg(m.nE, B, VV, eb, bk), s, m, B, bs, ut, ht, dd, ph));
+    return;
+  }
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, dd, ph)));
 }
 template <typename R, typename A>
@@ -222,8 +228,9 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
                                 tuned_v(K_TL_EDGE_TEND));
   const int bk = tuned_block(K_TL_EDGE_TEND);
   constexpr int J = BoundsNarrow::e2;
-  if (use_staged(m, B, v, eoe_stage_bytes<R, J, 3>(1), bk)) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eoe_stage_bytes<R, J, 3>(1), bk),
+  constexpr size_t eb = eoe_stage_bytes<R, J, 1, 3>();
+  if (use_staged(m, B, v, eb, bk)) {
+    MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eb, bk),
                                s, m, B, bs, ut, ht, d, ph, rk, tend_u));
     return;
   }
@@ -255,10 +262,33 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
                       cudaStream_t s) {
   g_launches++;
   switch (which) {
-    case 0: launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V)), tuned_block(K_AD_EDGE)), s, m, B, bs, ph, in, sd, w); break;
+    case 0: {
+      constexpr int J = BoundsNarrow::e2;
+      constexpr size_t eb = eoe_stage_bytes<R, J, 2, 3>();
+      const int bk = tuned_block(K_AD_EDGE);
+      if (use_staged(m, B, V, eb, bk))
+        launch_k(k_ad_edge_st<R, A, V, J>, staged_cfg(m.nE, B, V, eb, bk), s, m, B, bs, ph, in, sd, w);
+      else
+        launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
+      break;
+    }
     case 1: launch_k(k_ad_cell<R, A, V, NB>, launch_cfg((long long)(m.nC) * ((B) / (V)), tuned_block(K_AD_CELL)), s, m, B, bs, ph, in, sd, w); break;
     case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V)), tuned_block(K_AD_VERTEX)), s, m, B, bs, ph, in, sd, w); break;
-    case 3: launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), tuned_block(K_AD_FINAL)), s, m, B, bs, w, out); break;
+    case 3: {
+      constexpr int J = BoundsNarrow::e2;
+      constexpr size_t eb = eoe_stage_bytes<R, J, 2, 0>();
+      const int bk = tuned_block(K_AD_FINAL);
+      if (use_staged(m, B, V, eb, bk)) {
+        LaunchCfg c = staged_cfg(m.nE, B, V, eb, bk);
+        const long long cthreads = (long long)m.nC * (B / V);
+        const int cell_blocks = (int)((cthreads + c.block - 1) / c.block);
+        c.grid += cell_blocks;
+        launch_k(k_ad_final_st<R, A, V, J>, c, s, m, B, bs, w, out, cell_blocks);
+      } else {
+        launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), bk), s, m, B, bs, w, out);
+      }
+      break;
+    }
     case 4: launch_k(k_ad_del4_vc<R, V, NB>, launch_cfg((long long)(m.nV + m.nC) * ((B) / (V))), s, m, B, ph, in, w); break;
     default: launch_k(k_ad_del4_e<R, V>, launch_cfg((long long)(m.nE) * ((B) / (V))), s, m, B, w); break;
   }

@@ -156,6 +156,110 @@ __global__ void k_del4_vc(MeshDev<R> m, int B, const R *__restrict__ dsq_u, R *d
   }
 }
 
+// ---- edgesOnEdge lists ------------------------------------------------------------------
+// The edge kernels read the edgesOnEdge list of their edge through an accessor: slot j gives the
+// neighbour edge nb(j), weightsOnEdge w(j), its transpose wr(j) and linearisation-point fields at
+// the neighbour f(k, j).  EoeGlobal reads them from global memory; EoeShared from a block's
+// shared-memory copy (stage_eoe), so the member loads of every slot take their addresses from
+// shared memory instead of waiting on an index load from global memory.  Both give the same
+// values, so a kernel body computes the same numbers with either.
+template <typename R>
+struct EoeGlobal {
+  const int *eoe;
+  const R *wv, *wrv;
+  const R *fld[3];
+  int nE, e;
+  __device__ int nb(int j) const { return ld(eoe, (size_t)j * nE + e); }
+  __device__ R w(int j) const { return ld(wv, (size_t)j * nE + e); }
+  __device__ R wr(int j) const { return ld(wrv, (size_t)j * nE + e); }
+  __device__ R f(int k, int j) const { return ld(fld[k], nb(j)); }
+};
+template <typename R>
+__device__ __forceinline__ EoeGlobal<R> eoe_global(const MeshDev<R> &m, int e, const R *f0 = nullptr,
+                                                   const R *f1 = nullptr, const R *f2 = nullptr) {
+  EoeGlobal<R> g;
+  g.eoe = m.e_eoe;
+  g.wv = m.e_w;
+  g.wrv = m.e_wrev;
+  g.fld[0] = f0;
+  g.fld[1] = f1;
+  g.fld[2] = f2;
+  g.nE = m.nE;
+  g.e = e;
+  return g;
+}
+
+template <typename R>
+struct EoeShared {
+  const int *snb;
+  const R *sw, *swr, *sf;
+  int le, epb, J;
+  __device__ int at(int j) const { return j * epb + le; }
+  __device__ int nb(int j) const { return snb[at(j)]; }
+  __device__ R w(int j) const { return sw[at(j)]; }
+  __device__ R wr(int j) const { return swr[at(j)]; }
+  __device__ R f(int k, int j) const { return sf[(size_t)k * J * epb + at(j)]; }
+};
+
+// Shared-memory bytes per edge of a stage with HW weights arrays (0-2) and NF fields.
+template <typename R, int J, int HW, int NF>
+constexpr size_t eoe_stage_bytes() {
+  return (size_t)J * (sizeof(int) + (HW + NF) * sizeof(R));
+}
+
+// Copy the lists of edges e0 .. e0 + epb - 1 into shared memory (weights: e_w if HW >= 1, e_wrev
+// if HW == 2; fields[k] at the neighbours) with coalesced slot-major loads spread over the block,
+// then __syncthreads.  Every thread of the block must call it; le selects the caller's edge.
+template <typename R, int J, int HW, int NF>
+__device__ EoeShared<R> stage_eoe(const MeshDev<R> &m, int e0, int epb, int le, const R *const *fields) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sw = reinterpret_cast<R *>(smem_raw);
+  R *swr = sw + (HW >= 1 ? (size_t)J * epb : 0);
+  R *sf = swr + (HW >= 2 ? (size_t)J * epb : 0);
+  int *snb = reinterpret_cast<int *>(sf + (size_t)NF * J * epb);
+  const int nE = m.nE;
+  for (int i = threadIdx.x; i < J * epb; i += blockDim.x) {
+    const int j = i / epb, l = i - j * epb, e = e0 + l;
+    int nb = 0;
+    R w = R(0), wr = R(0);
+    R f[NF > 0 ? NF : 1];
+#pragma unroll
+    for (int k = 0; k < NF; k++) f[k] = R(0);
+    if (e < nE && j < ld(m.e_n, e)) {
+      nb = ld(m.e_eoe, (size_t)j * nE + e);
+      if (HW >= 1) w = ld(m.e_w, (size_t)j * nE + e);
+      if (HW >= 2) wr = ld(m.e_wrev, (size_t)j * nE + e);
+#pragma unroll
+      for (int k = 0; k < NF; k++) f[k] = ld(fields[k], nb);
+    }
+    snb[i] = nb;
+    if (HW >= 1) sw[i] = w;
+    if (HW >= 2) swr[i] = wr;
+#pragma unroll
+    for (int k = 0; k < NF; k++) sf[(size_t)k * J * epb + i] = f[k];
+  }
+  __syncthreads();
+  EoeShared<R> st;
+  st.snb = snb;
+  st.sw = sw;
+  st.swr = swr;
+  st.sf = sf;
+  st.le = le;
+  st.epb = epb;
+  st.J = J;
+  return st;
+}
+
+// The thread's edge and first member in a staged edge kernel (blocks of epb edges with B / V
+// threads each); false for threads past the last edge.
+__device__ __forceinline__ bool staged_edge(int nE, int B, int V, int *le, int *e, int *b) {
+  const int tpe = B / V;
+  *le = threadIdx.x / tpe;
+  *e = blockIdx.x * (blockDim.x / tpe) + *le;
+  *b = (threadIdx.x - *le * tpe) * V;
+  return *le < (int)(blockDim.x / tpe) && *e < nE;
+}
+
 // ----------------------------------------------------------------------------------------
 // Tangent linear (src/mpas_sw_dyncore_tlm.f90)
 // ----------------------------------------------------------------------------------------
@@ -243,183 +347,76 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_tl_cell(MeshDev
   }
 }
 
-// :319-329, :364-393, :425-445, h_edge_tl :117-126, delsq_u_tl :638-652
+// :319-329, :364-393, :425-445, h_edge_tl :117-126, delsq_u_tl :638-652.  Body for edge e,
+// members b .. b+V-1; l is the edge's edgesOnEdge list.
+template <typename R, int V, int NMAX, class L>
+__device__ __forceinline__ void tl_edge_diag_body(const MeshDev<R> &m, int B, const Base<R> &bs,
+                                                  const R *__restrict__ ut, const R *__restrict__ ht,
+                                                  const Diag<R> &d, const Phys<R> &ph, int e, int b, const L &l) {
+  using M = Mv<R, V>;
+  const int n = ld(m.e_n, e);
+  M vt = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(j, NMAX, n)
+    vt = vt + l.w(j) * ldv<V>(ut + (size_t)l.nb(j) * B + b);
+  const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
+  const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
+  const M gptt = (ldv<V>(d.pvv + (size_t)v2 * B + b) - ldv<V>(d.pvv + (size_t)v1 * B + b)) / dv;
+  M pet = mv_fill<R, V>(R(0));
+  pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_va, e) * B + b);
+  pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_vb, e) * B + b);
+  pet = pet - ((ph.apvm * vt) * ph.dt) * ld(bs.gpt, e) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * gptt;
+  const M gpnt = (ldv<V>(d.pc + (size_t)c2 * B + b) - ldv<V>(d.pc + (size_t)c1 * B + b)) / dc;
+  const M uet = ldv<V>(ut + (size_t)e * B + b);
+  pet = pet - ((ph.apvm * uet) * ph.dt) * ld(bs.gpn, e) - ((ph.apvm * ld(bs.u, e)) * ph.dt) * gpnt;
+  const size_t o = (size_t)e * B + b;
+  stv<V>(d.pe + o, pet);
+  stv<V>(d.he + o, R(0.5) * (ldv<V>(ht + (size_t)c1 * B + b) + ldv<V>(ht + (size_t)c2 * B + b)));
+  if (d.v) stv<V>(d.v + o, vt);
+  if (d.gpt) stv<V>(d.gpt + o, gptt);
+  if (d.gpn) stv<V>(d.gpn + o, gpnt);
+  if (d.dsq_u)
+    stv<V>(d.dsq_u + o, (ldv<V>(d.div + (size_t)c2 * B + b) - ldv<V>(d.div + (size_t)c1 * B + b)) / dc -
+                            (ldv<V>(d.vort + (size_t)v2 * B + b) - ldv<V>(d.vort + (size_t)v1 * B + b)) / dv);
+}
+
 template <typename R, int V, class NB>
 __global__ void k_tl_edge_diag(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                                const R *__restrict__ ht, Diag<R> d, Phys<R> ph) {
-  using M = Mv<R, V>;
-  const int nE = m.nE;
-  MPSW_MEMBER_LOOP(t, nE, B, V) {
+  MPSW_MEMBER_LOOP(t, m.nE, B, V) {
     const EntMember q = ent_member(t, B, V);
-    const int e = q.ent;
-    const int n = ld(m.e_n, e);
-    M vt = mv_fill<R, V>(R(0));
-    MPSW_SLOTS(j, NB::e2, n)
-      vt = vt + ld(m.e_w, (size_t)j * nE + e) * ldv<V>(ut + (size_t)ld(m.e_eoe, (size_t)j * nE + e) * B + q.b);
-    const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
-    const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
-    const M gptt = (ldv<V>(d.pvv + (size_t)v2 * B + q.b) - ldv<V>(d.pvv + (size_t)v1 * B + q.b)) / dv;
-    M pet = mv_fill<R, V>(R(0));
-    pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_va, e) * B + q.b);
-    pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_vb, e) * B + q.b);
-    pet = pet - ((ph.apvm * vt) * ph.dt) * ld(bs.gpt, e) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * gptt;
-    const M gpnt = (ldv<V>(d.pc + (size_t)c2 * B + q.b) - ldv<V>(d.pc + (size_t)c1 * B + q.b)) / dc;
-    const M uet = ldv<V>(ut + (size_t)e * B + q.b);
-    pet = pet - ((ph.apvm * uet) * ph.dt) * ld(bs.gpn, e) - ((ph.apvm * ld(bs.u, e)) * ph.dt) * gpnt;
-    const size_t o = (size_t)e * B + q.b;
-    stv<V>(d.pe + o, pet);
-    stv<V>(d.he + o, R(0.5) * (ldv<V>(ht + (size_t)c1 * B + q.b) + ldv<V>(ht + (size_t)c2 * B + q.b)));
-    if (d.v) stv<V>(d.v + o, vt);
-    if (d.gpt) stv<V>(d.gpt + o, gptt);
-    if (d.gpn) stv<V>(d.gpn + o, gpnt);
-    if (d.dsq_u)
-      stv<V>(d.dsq_u + o, (ldv<V>(d.div + (size_t)c2 * B + q.b) - ldv<V>(d.div + (size_t)c1 * B + q.b)) / dc -
-                              (ldv<V>(d.vort + (size_t)v2 * B + q.b) - ldv<V>(d.vort + (size_t)v1 * B + q.b)) / dv);
+    tl_edge_diag_body<R, V, NB::e2>(m, B, bs, ut, ht, d, ph, q.ent, q.b, eoe_global(m, q.ent));
   }
 }
 
-// sw_compute_tend_tlm normal-velocity part :564-768 and the RK update
-template <typename R, typename A, int V, class NB>
-__global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
-                               const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
-                               R *tend_u) {
-  using M = Mv<R, V>;
-  const int nE = m.nE;
-  MPSW_MEMBER_LOOP(t, nE, B, V) {
-    const EntMember q = ent_member(t, B, V);
-    const int e = q.ent;
-    const int n = ld(m.e_n, e);
-    const M pet_e = ldv<V>(d.pe + (size_t)e * B + q.b);
-    const R pe_e = ld(bs.pe, e);
-    M qt = mv_fill<R, V>(R(0));
-    MPSW_SLOTS(j, NB::e2, n) {
-      const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
-      const R w = ld(m.e_w, (size_t)j * nE + e);
-      const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + q.b));
-      const R wpv = R(0.5) * (pe_e + ld(bs.pe, eoe));
-      const R ub = ld(bs.u, eoe), heb = ld(bs.he, eoe);
-      qt = qt + ((w * ldv<V>(ut + (size_t)eoe * B + q.b)) * wpv) * heb + ((w * ub) * wpvt) * heb +
-           ((w * ub) * wpv) * ldv<V>(d.he + (size_t)eoe * B + q.b);
-    }
-    const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
-    const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
-    M tut = qt - ((ldv<V>(d.ke + (size_t)c2 * B + q.b) - ldv<V>(d.ke + (size_t)c1 * B + q.b)) +
-                  R(GRAVITY) * (ldv<V>(ht + (size_t)c2 * B + q.b) - ldv<V>(ht + (size_t)c1 * B + q.b))) / dc;
-    if (ph.visc2 > R(0)) {
-      M ud = (ldv<V>(d.div + (size_t)c2 * B + q.b) - ldv<V>(d.div + (size_t)c1 * B + q.b)) / dc -
-             (ldv<V>(d.vort + (size_t)v2 * B + q.b) - ldv<V>(d.vort + (size_t)v1 * B + q.b)) / dv;
-      ud = (ld(m.e_sc2, e) * ph.visc2) * ud;
-      tut = tut + ud;
-    }
-    if (ph.visc4 > R(0)) {
-      M ud = (ldv<V>(d.dsq_div + (size_t)c2 * B + q.b) - ldv<V>(d.dsq_div + (size_t)c1 * B + q.b)) / dc -
-             (ldv<V>(d.dsq_vort + (size_t)v2 * B + q.b) - ldv<V>(d.dsq_vort + (size_t)v1 * B + q.b)) / dv;
-      ud = (ld(m.e_sc4, e) * ph.visc4) * ud;
-      tut = tut - ud;
-    }
-    const R hh = ld(bs.he, e);
-    const M het = ldv<V>(d.he + (size_t)e * B + q.b);
-    if (ph.wind) tut = tut - ((het * ld(m.e_usrc, e)) / R(RHO_REF)) / (hh * hh);
-    if (ph.drag) {
-      const M ket_e = R(0.5) * (ldv<V>(d.ke + (size_t)c1 * B + q.b) + ldv<V>(d.ke + (size_t)c2 * B + q.b));
-      const R ke_e = R(0.5) * (ld(bs.ke, c1) + ld(bs.ke, c2));
-      const R uu = ld(bs.u, e), sq = sqrt(R(2) * ke_e);
-      tut = tut - ((R(1.0e-3) * ldv<V>(ut + (size_t)e * B + q.b)) * sq) / hh -
-            ((((R(0.5) * R(1.0e-3)) * uu) * (R(2) * ket_e)) / sq) / hh +
-            (((R(1.0e-3) * uu) * sq) * het) / (hh * hh);
-    }
-    const size_t o = (size_t)e * B + q.b;
-    if (tend_u) stv<V>(tend_u + o, tut);
-    rk_members<R, A, V>(rk, o, tut);
-  }
-}
-
-// ---- edgesOnEdge lists staged in shared memory --------------------------------------------
-// A block of the staged edge kernels handles `epb` consecutive edges with B / V threads each.
-// Before the member work, the block copies the edgesOnEdge lists of its edges (neighbour index,
-// weight and up to three per-edge fields of the linearisation point at the neighbour) into
-// shared memory, slot-major ([J][epb]), with coalesced loads spread over all its threads; the
-// member loads of every slot then take their addresses from shared memory, so each thread's
-// loads no longer wait on an index load from global memory first.
-template <typename R, int J, int NF>
-struct EoeStage {
-  const int *nb;      // [J][epb] neighbour edge (0 past the edge's list)
-  const R *w;         // [J][epb] weight (0 past the list)
-  const R *f[NF];     // [J][epb] field k at the neighbour
-  int epb;
-  __device__ int at(int j, int le) const { return j * epb + le; }
-};
-
-// Shared-memory bytes of an EoeStage for `epb` edges.
-template <typename R, int J, int NF>
-constexpr size_t eoe_stage_bytes(int epb) {
-  return (size_t)J * epb * (sizeof(int) + (1 + NF) * sizeof(R));
-}
-
-// Fill the stage of edges e0 .. e0 + epb - 1 (weights from `wts`: weightsOnEdge or its transpose)
-// and __syncthreads.  Every thread of the block must call it.
-template <typename R, int J, int NF>
-__device__ EoeStage<R, J, NF> stage_eoe(const MeshDev<R> &m, const R *wts, int e0, int epb,
-                                        const R *const (&fields)[NF]) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *sw = reinterpret_cast<R *>(smem_raw);
-  R *sf = sw + (size_t)J * epb;
-  int *snb = reinterpret_cast<int *>(sf + (size_t)NF * J * epb);
-  const int nE = m.nE;
-  for (int i = threadIdx.x; i < J * epb; i += blockDim.x) {
-    const int j = i / epb, le = i - j * epb, e = e0 + le;
-    int nb = 0;
-    R w = R(0);
-    R f[NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) f[k] = R(0);
-    if (e < nE && j < ld(m.e_n, e)) {
-      nb = ld(m.e_eoe, (size_t)j * nE + e);
-      w = ld(wts, (size_t)j * nE + e);
-#pragma unroll
-      for (int k = 0; k < NF; k++) f[k] = ld(fields[k], nb);
-    }
-    snb[i] = nb;
-    sw[i] = w;
-#pragma unroll
-    for (int k = 0; k < NF; k++) sf[(size_t)k * J * epb + i] = f[k];
-  }
-  __syncthreads();
-  EoeStage<R, J, NF> st;
-  st.nb = snb;
-  st.w = sw;
-#pragma unroll
-  for (int k = 0; k < NF; k++) st.f[k] = sf + (size_t)k * J * epb;
-  st.epb = epb;
-  return st;
-}
-
-// k_tl_edge_tend with staged edgesOnEdge lists: one block per `epb` edges, no grid-stride loop.
-template <typename R, typename A, int V, int J>
-__global__ void k_tl_edge_tend_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
-                                  const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
-                                  R *tend_u) {
-  using M = Mv<R, V>;
+template <typename R, int V, int J>
+__global__ void k_tl_edge_diag_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                                  const R *__restrict__ ht, Diag<R> d, Phys<R> ph) {
   pdl_begin();
-  const int tpe = B / V, epb = blockDim.x / tpe;
-  const int e0 = blockIdx.x * epb;
-  const R *const fields[3] = {bs.pe, bs.u, bs.he};
-  const EoeStage<R, J, 3> st = stage_eoe<R, J, 3>(m, m.e_w, e0, epb, fields);
-  const int le = threadIdx.x / tpe;
-  const int e = e0 + le;
-  if (le >= epb || e >= m.nE) return;
-  const int b = (threadIdx.x - le * tpe) * V;
+  int le, e, b;
+  const bool mine = staged_edge(m.nE, B, V, &le, &e, &b);
+  const int epb = blockDim.x / (B / V);
+  const EoeShared<R> st = stage_eoe<R, J, 1, 0>(m, blockIdx.x * epb, epb, le, nullptr);
+  if (mine) tl_edge_diag_body<R, V, J>(m, B, bs, ut, ht, d, ph, e, b, st);
+}
+
+// sw_compute_tend_tlm normal-velocity part :564-768 and the RK update.  Body for edge e,
+// members b .. b+V-1; l is the edge's edgesOnEdge list with fields pv_edge, u, h_edge.
+template <typename R, typename A, int V, int NMAX, class L>
+__device__ __forceinline__ void tl_edge_tend_body(const MeshDev<R> &m, int B, const Base<R> &bs,
+                                                  const R *__restrict__ ut, const R *__restrict__ ht,
+                                                  const Diag<R> &d, const Phys<R> &ph, const RK<R, A> &rk,
+                                                  R *tend_u, int e, int b, const L &l) {
+  using M = Mv<R, V>;
   const int n = ld(m.e_n, e);
   const M pet_e = ldv<V>(d.pe + (size_t)e * B + b);
   const R pe_e = ld(bs.pe, e);
   M qt = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(j, J, n) {
-    const int i = st.at(j, le);
-    const int eoe = st.nb[i];
-    const R w = st.w[i];
+  MPSW_SLOTS(j, NMAX, n) {
+    const int eoe = l.nb(j);
+    const R w = l.w(j);
     const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + b));
-    const R wpv = R(0.5) * (pe_e + st.f[0][i]);
-    const R ub = st.f[1][i], heb = st.f[2][i];
+    const R wpv = R(0.5) * (pe_e + l.f(0, j));
+    const R ub = l.f(1, j), heb = l.f(2, j);
     qt = qt + ((w * ldv<V>(ut + (size_t)eoe * B + b)) * wpv) * heb + ((w * ub) * wpvt) * heb +
          ((w * ub) * wpv) * ldv<V>(d.he + (size_t)eoe * B + b);
   }
@@ -453,6 +450,31 @@ __global__ void k_tl_edge_tend_st(MeshDev<R> m, int B, Base<R> bs, const R *__re
   const size_t o = (size_t)e * B + b;
   if (tend_u) stv<V>(tend_u + o, tut);
   rk_members<R, A, V>(rk, o, tut);
+}
+
+template <typename R, typename A, int V, class NB>
+__global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                               const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
+                               R *tend_u) {
+  MPSW_MEMBER_LOOP(t, m.nE, B, V) {
+    const EntMember q = ent_member(t, B, V);
+    tl_edge_tend_body<R, A, V, NB::e2>(m, B, bs, ut, ht, d, ph, rk, tend_u, q.ent, q.b,
+                                       eoe_global(m, q.ent, bs.pe, bs.u, bs.he));
+  }
+}
+
+// k_tl_edge_tend with the edgesOnEdge lists staged in shared memory: one block per epb edges.
+template <typename R, typename A, int V, int J>
+__global__ void k_tl_edge_tend_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                                  const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
+                                  R *tend_u) {
+  pdl_begin();
+  int le, e, b;
+  const bool mine = staged_edge(m.nE, B, V, &le, &e, &b);
+  const int epb = blockDim.x / (B / V);
+  const R *const fields[3] = {bs.pe, bs.u, bs.he};
+  const EoeShared<R> st = stage_eoe<R, J, 1, 3>(m, blockIdx.x * epb, epb, le, fields);
+  if (mine) tl_edge_tend_body<R, A, V, J>(m, B, bs, ut, ht, d, ph, rk, tend_u, e, b, st);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -498,58 +520,77 @@ __global__ void k_ad_tinit(MeshDev<R> m, int B, const A *x2u, const A *x2h, cons
 // Edge stage: workpv/q adjoint (:689-718) as a gather over the transposed edgesOnEdge,
 // thickness-flux adjoint (:720-736), drag (:549-565), wind (:567-572), then the APVM adjoints
 // of the diagnostics (:193-200, :235-242).
+template <typename R, typename A, int V, int NMAX, class L>
+__device__ __forceinline__ void ad_edge_body(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
+                                             const AdIn<R> &in, const AdSeeds<R> &sd, const AdWork<R> &w, int e,
+                                             int b, const L &l) {
+  using M = Mv<R, V>;
+  const int n = ld(m.e_n, e);
+  const M Te = ldv<V>(in.tu + (size_t)e * B + b);
+  const R ue = ld(bs.u, e), hee = ld(bs.he, e), pee = ld(bs.pe, e);
+  M pe_ad = mv_fill<R, V>(R(0)), he_ad = mv_fill<R, V>(R(0)), ud = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(j, NMAX, n) {
+    const int nb = l.nb(j);
+    const R wj = l.w(j);
+    const R wr = l.wr(j);
+    pe_ad = pe_ad + R(0.5) * (((wj * l.f(0, j)) * l.f(1, j)) * Te);
+    const M Tn = ldv<V>(in.tu + (size_t)nb * B + b);
+    const R wpv = R(0.5) * (l.f(2, j) + pee);
+    he_ad = he_ad + ((wr * ue) * wpv) * Tn;
+    pe_ad = pe_ad + R(0.5) * (((wr * ue) * hee) * Tn);
+    ud = ud + ((wr * wpv) * hee) * Tn;
+  }
+  const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
+  const R dv = ld(m.e_dv, e);
+  const M fa = ldv<V>(in.th + (size_t)c2 * B + b) - ldv<V>(in.th + (size_t)c1 * B + b);
+  he_ad = he_ad + (ue * dv) * fa;
+  ud = ud + (dv * hee) * fa;
+  if (ph.drag) {
+    const R sq = sqrt(R(2) * (R(0.5) * (ld(bs.ke, c1) + ld(bs.ke, c2))));
+    he_ad = he_ad + (((R(1.0e-3) * ue) * sq) / (hee * hee)) * Te;
+    ud = ud - ((R(1.0e-3) * sq) / hee) * Te;
+  }
+  if (ph.wind) he_ad = he_ad - ((ld(m.e_usrc, e) / R(RHO_REF)) / (hee * hee)) * Te;
+  M gpn_ad = mv_fill<R, V>(R(0)), gpt_ad = mv_fill<R, V>(R(0)), v_ad = mv_fill<R, V>(R(0));
+  if (sd.pe) pe_ad = pe_ad + sd.pe[e];
+  if (sd.he) he_ad = he_ad + sd.he[e];
+  if (sd.gpn) gpn_ad = mv_fill<R, V>(sd.gpn[e]);
+  if (sd.gpt) gpt_ad = mv_fill<R, V>(sd.gpt[e]);
+  if (sd.v) v_ad = mv_fill<R, V>(sd.v[e]);
+  gpn_ad = gpn_ad - ((ph.apvm * ue) * ph.dt) * pe_ad;
+  ud = ud - ((ph.apvm * ph.dt) * ld(bs.gpn, e)) * pe_ad;
+  gpt_ad = gpt_ad - ((ph.apvm * ld(bs.v, e)) * ph.dt) * pe_ad;
+  v_ad = v_ad - ((ph.apvm * ph.dt) * ld(bs.gpt, e)) * pe_ad;
+  const size_t o = (size_t)e * B + b;
+  stv<V>(w.pe_ad + o, pe_ad);
+  stv<V>(w.he_ad + o, he_ad);
+  stv<V>(w.ud + o, ud);
+  stv<V>(w.gpn_ad + o, gpn_ad);
+  stv<V>(w.gpt_ad + o, gpt_ad);
+  stv<V>(w.v_ad + o, v_ad);
+}
+
 template <typename R, typename A, int V, class NB>
 __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                           AdWork<R> w) {
-  using M = Mv<R, V>;
-  const int nE = m.nE;
-  MPSW_MEMBER_LOOP(t, nE, B, V) {
+  MPSW_MEMBER_LOOP(t, m.nE, B, V) {
     const EntMember q = ent_member(t, B, V);
-    const int e = q.ent;
-    const int n = ld(m.e_n, e);
-    const M Te = ldv<V>(in.tu + (size_t)e * B + q.b);
-    const R ue = ld(bs.u, e), hee = ld(bs.he, e), pee = ld(bs.pe, e);
-    M pe_ad = mv_fill<R, V>(R(0)), he_ad = mv_fill<R, V>(R(0)), ud = mv_fill<R, V>(R(0));
-    MPSW_SLOTS(j, NB::e2, n) {
-      const int nb = ld(m.e_eoe, (size_t)j * nE + e);
-      const R wj = ld(m.e_w, (size_t)j * nE + e);
-      const R wr = ld(m.e_wrev, (size_t)j * nE + e);
-      pe_ad = pe_ad + R(0.5) * (((wj * ld(bs.u, nb)) * ld(bs.he, nb)) * Te);
-      const M Tn = ldv<V>(in.tu + (size_t)nb * B + q.b);
-      const R wpv = R(0.5) * (ld(bs.pe, nb) + pee);
-      he_ad = he_ad + ((wr * ue) * wpv) * Tn;
-      pe_ad = pe_ad + R(0.5) * (((wr * ue) * hee) * Tn);
-      ud = ud + ((wr * wpv) * hee) * Tn;
-    }
-    const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
-    const R dv = ld(m.e_dv, e);
-    const M fa = ldv<V>(in.th + (size_t)c2 * B + q.b) - ldv<V>(in.th + (size_t)c1 * B + q.b);
-    he_ad = he_ad + (ue * dv) * fa;
-    ud = ud + (dv * hee) * fa;
-    if (ph.drag) {
-      const R sq = sqrt(R(2) * (R(0.5) * (ld(bs.ke, c1) + ld(bs.ke, c2))));
-      he_ad = he_ad + (((R(1.0e-3) * ue) * sq) / (hee * hee)) * Te;
-      ud = ud - ((R(1.0e-3) * sq) / hee) * Te;
-    }
-    if (ph.wind) he_ad = he_ad - ((ld(m.e_usrc, e) / R(RHO_REF)) / (hee * hee)) * Te;
-    M gpn_ad = mv_fill<R, V>(R(0)), gpt_ad = mv_fill<R, V>(R(0)), v_ad = mv_fill<R, V>(R(0));
-    if (sd.pe) pe_ad = pe_ad + sd.pe[e];
-    if (sd.he) he_ad = he_ad + sd.he[e];
-    if (sd.gpn) gpn_ad = mv_fill<R, V>(sd.gpn[e]);
-    if (sd.gpt) gpt_ad = mv_fill<R, V>(sd.gpt[e]);
-    if (sd.v) v_ad = mv_fill<R, V>(sd.v[e]);
-    gpn_ad = gpn_ad - ((ph.apvm * ue) * ph.dt) * pe_ad;
-    ud = ud - ((ph.apvm * ph.dt) * ld(bs.gpn, e)) * pe_ad;
-    gpt_ad = gpt_ad - ((ph.apvm * ld(bs.v, e)) * ph.dt) * pe_ad;
-    v_ad = v_ad - ((ph.apvm * ph.dt) * ld(bs.gpt, e)) * pe_ad;
-    const size_t o = (size_t)e * B + q.b;
-    stv<V>(w.pe_ad + o, pe_ad);
-    stv<V>(w.he_ad + o, he_ad);
-    stv<V>(w.ud + o, ud);
-    stv<V>(w.gpn_ad + o, gpn_ad);
-    stv<V>(w.gpt_ad + o, gpt_ad);
-    stv<V>(w.v_ad + o, v_ad);
+    ad_edge_body<R, A, V, NB::e2>(m, B, bs, ph, in, sd, w, q.ent, q.b, eoe_global(m, q.ent, bs.u, bs.he, bs.pe));
   }
+}
+
+// k_ad_edge with the edgesOnEdge lists (both weights; u, h_edge, pv_edge at the neighbours)
+// staged in shared memory: one block per epb edges.
+template <typename R, typename A, int V, int J>
+__global__ void k_ad_edge_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+                             AdWork<R> w) {
+  pdl_begin();
+  int le, e, b;
+  const bool mine = staged_edge(m.nE, B, V, &le, &e, &b);
+  const int epb = blockDim.x / (B / V);
+  const R *const fields[3] = {bs.u, bs.he, bs.pe};
+  const EoeShared<R> st = stage_eoe<R, J, 2, 3>(m, blockIdx.x * epb, epb, le, fields);
+  if (mine) ad_edge_body<R, A, V, J>(m, B, bs, ph, in, sd, w, e, b, st);
 }
 
 // del4 adjoint, first half (:588-634): delsq_vorticity/delsq_circulation adjoint on vertices
@@ -763,41 +804,71 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
 // Final stage of the adjoint: h_vertex -> h (:286-289) on cells, and on edges the transposed
 // tangential velocity (:296-303), ke (:306-317), divergence (:327-340) and circulation
 // (:350-355) adjoints.  Cell threads then edge threads.
+template <typename R, typename A, int V, int NMAX>
+__device__ __forceinline__ void ad_final_cell(const MeshDev<R> &m, int B, const AdWork<R> &w,
+                                              const AdOut<R, A> &out, int c, int b) {
+  using M = Mv<R, V>;
+  const int nC = m.nC;
+  const int n = ld(m.c_n, c);
+  M ph_ = ldv<V>(w.hd + (size_t)c * B + b);
+  MPSW_SLOTS(k, NMAX, n)
+    ph_ = ph_ + ld(m.c_vk, (size_t)k * nC + c) * ldv<V>(w.hv_ad + (size_t)ld(m.c_vs, (size_t)k * nC + c) * B + b);
+  ad_emit<R, A, V>(out, 0, (size_t)c * B + b, ph_, ld(m.c_area, c));
+}
+
+template <typename R, typename A, int V, int NMAX, class L>
+__device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const Base<R> &bs, const AdWork<R> &w,
+                                              const AdOut<R, A> &out, int e, int b, const L &l) {
+  using M = Mv<R, V>;
+  const int n = ld(m.e_n, e);
+  M pu = ldv<V>(w.ud + (size_t)e * B + b);
+  MPSW_SLOTS(j, NMAX, n)
+    pu = pu + l.wr(j) * ldv<V>(w.v_ad + (size_t)l.nb(j) * B + b);
+  const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
+  const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
+  const R kc = (((R(0.25) * dc) * dv) * R(2)) * ld(bs.u, e);
+  pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c1 * B + b);
+  pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c2 * B + b);
+  pu = pu - dv * ldv<V>(w.div_ad + (size_t)c2 * B + b);
+  pu = pu + dv * ldv<V>(w.div_ad + (size_t)c1 * B + b);
+  pu = pu + dc * ldv<V>(w.circ_ad + (size_t)v2 * B + b);
+  pu = pu - dc * ldv<V>(w.circ_ad + (size_t)v1 * B + b);
+  ad_emit<R, A, V>(out, 1, (size_t)e * B + b, pu, R(1));
+}
+
 template <typename R, typename A, int V, class NB>
 __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out) {
-  using M = Mv<R, V>;
-  const int nC = m.nC, nE = m.nE;
-  const long long tc = (long long)nC * (B / V);
-  MPSW_GRID_LOOP(t, tc + (long long)nE * (B / V)) {
+  const long long tc = (long long)m.nC * (B / V);
+  MPSW_GRID_LOOP(t, tc + (long long)m.nE * (B / V)) {
     if (t < tc) {
       const EntMember q = ent_member(t, B, V);
-      const int c = q.ent;
-      const int n = ld(m.c_n, c);
-      M ph_ = ldv<V>(w.hd + (size_t)c * B + q.b);
-      MPSW_SLOTS(k, NB::c, n)
-        ph_ = ph_ + ld(m.c_vk, (size_t)k * nC + c) * ldv<V>(w.hv_ad + (size_t)ld(m.c_vs, (size_t)k * nC + c) * B + q.b);
-      ad_emit<R, A, V>(out, 0, (size_t)c * B + q.b, ph_, ld(m.c_area, c));
+      ad_final_cell<R, A, V, NB::c>(m, B, w, out, q.ent, q.b);
     } else {
       const EntMember q = ent_member(t - tc, B, V);
-      const int e = q.ent;
-      const int n = ld(m.e_n, e);
-      M pu = ldv<V>(w.ud + (size_t)e * B + q.b);
-      MPSW_SLOTS(j, NB::e2, n) {
-        const int nb = ld(m.e_eoe, (size_t)j * nE + e);
-        pu = pu + ld(m.e_wrev, (size_t)j * nE + e) * ldv<V>(w.v_ad + (size_t)nb * B + q.b);
-      }
-      const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
-      const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
-      const R kc = (((R(0.25) * dc) * dv) * R(2)) * ld(bs.u, e);
-      pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c1 * B + q.b);
-      pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c2 * B + q.b);
-      pu = pu - dv * ldv<V>(w.div_ad + (size_t)c2 * B + q.b);
-      pu = pu + dv * ldv<V>(w.div_ad + (size_t)c1 * B + q.b);
-      pu = pu + dc * ldv<V>(w.circ_ad + (size_t)v2 * B + q.b);
-      pu = pu - dc * ldv<V>(w.circ_ad + (size_t)v1 * B + q.b);
-      ad_emit<R, A, V>(out, 1, (size_t)e * B + q.b, pu, R(1));
+      ad_final_edge<R, A, V, NB::e2>(m, B, bs, w, out, q.ent, q.b, eoe_global(m, q.ent));
     }
   }
+}
+
+// k_ad_final with staged edge lists: the first cell_blocks blocks take the cells (one member
+// group per thread), the others epb edges each with their lists in shared memory.
+template <typename R, typename A, int V, int J>
+__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out, int cell_blocks) {
+  pdl_begin();
+  if ((int)blockIdx.x < cell_blocks) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (long long)m.nC * (B / V)) {
+      const EntMember q = ent_member(t, B, V);
+      ad_final_cell<R, A, V, BoundsNarrow::c>(m, B, w, out, q.ent, q.b);
+    }
+    return;
+  }
+  const int tpe = B / V, epb = blockDim.x / tpe;
+  const int le = threadIdx.x / tpe;
+  const int e = ((int)blockIdx.x - cell_blocks) * epb + le;
+  const int b = (threadIdx.x - le * tpe) * V;
+  const EoeShared<R> st = stage_eoe<R, J, 2, 0>(m, ((int)blockIdx.x - cell_blocks) * epb, epb, le, nullptr);
+  if (le < epb && e < m.nE) ad_final_edge<R, A, V, J>(m, B, bs, w, out, e, b, st);
 }
 
 }  // namespace mpsw
