@@ -6,6 +6,7 @@ namespace mpsw {
 
 long long g_launches = 0;
 thread_local const TuneTable *g_tune = nullptr;
+thread_local bool g_stable_base = false;
 
 int grid_for(long long total) {
   long long g = (total + kThreads - 1) / kThreads;

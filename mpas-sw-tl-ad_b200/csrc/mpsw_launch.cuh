@@ -212,7 +212,7 @@ void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, c
   constexpr int J = BoundsNarrow::e2;
   constexpr size_t eb = eoe_stage_bytes<R, J, 1, 0>();
   if (use_staged(m, B, v, eb, bk)) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_edge_diag_st<R, VV, J>, staged_cfg(m.nE, B, VV, eb, bk), s, m, B, bs, ut, ht, dd, ph));
+    MPSW_VDISPATCH(v, launch_k(k_tl_edge_diag_st<R, VV, J>, staged_cfg(m.nE, B, VV, eb, bk), s, m, B, bs, ut, ht, dd, ph, (int)g_stable_base));
     return;
   }
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, dd, ph)));
@@ -231,7 +231,7 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
   constexpr size_t eb = eoe_stage_bytes<R, J, 1, 3>();
   if (use_staged(m, B, v, eb, bk)) {
     MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eb, bk),
-                               s, m, B, bs, ut, ht, d, ph, rk, tend_u));
+                               s, m, B, bs, ut, ht, d, ph, rk, tend_u, (int)g_stable_base));
     return;
   }
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_tend<R, A, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, d, ph, rk, tend_u)));
@@ -267,7 +267,7 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
       constexpr size_t eb = eoe_stage_bytes<R, J, 2, 3>();
       const int bk = tuned_block(K_AD_EDGE);
       if (use_staged(m, B, V, eb, bk))
-        launch_k(k_ad_edge_st<R, A, V, J>, staged_cfg(m.nE, B, V, eb, bk), s, m, B, bs, ph, in, sd, w);
+        launch_k(k_ad_edge_st<R, A, V, J>, staged_cfg(m.nE, B, V, eb, bk), s, m, B, bs, ph, in, sd, w, (int)g_stable_base);
       else
         launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
       break;
@@ -283,7 +283,7 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
         const long long cthreads = (long long)m.nC * (B / V);
         const int cell_blocks = (int)((cthreads + c.block - 1) / c.block);
         c.grid += cell_blocks;
-        launch_k(k_ad_final_st<R, A, V, J>, c, s, m, B, bs, w, out, cell_blocks);
+        launch_k(k_ad_final_st<R, A, V, J>, c, s, m, B, bs, w, out, cell_blocks, (int)g_stable_base);
       } else {
         launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), bk), s, m, B, bs, w, out);
       }

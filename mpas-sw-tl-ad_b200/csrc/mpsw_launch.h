@@ -33,6 +33,16 @@ struct TuneScope {
   ~TuneScope() { g_tune = prev; }
 };
 
+// Set while launching a sweep in which no kernel writes the mesh or the linearisation points
+// (sweeps over stored stages): the staged kernels then copy their neighbour lists into shared
+// memory before waiting for the previous kernel, overlapping that copy with its tail.
+extern thread_local bool g_stable_base;
+struct StableBaseScope {
+  bool prev;
+  explicit StableBaseScope(bool on) : prev(g_stable_base) { g_stable_base = on; }
+  ~StableBaseScope() { g_stable_base = prev; }
+};
+
 template <typename R, typename A>
 struct Launch {
   // forward stage pieces (single trajectory)

@@ -390,12 +390,13 @@ __global__ void k_tl_edge_diag(MeshDev<R> m, int B, Base<R> bs, const R *__restr
 
 template <typename R, int V, int J>
 __global__ void k_tl_edge_diag_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
-                                  const R *__restrict__ ht, Diag<R> d, Phys<R> ph) {
-  pdl_begin();
+                                  const R *__restrict__ ht, Diag<R> d, Phys<R> ph, int early) {
+  if (!early) pdl_begin();
   int le, e, b;
   const bool mine = staged_edge(m.nE, B, V, &le, &e, &b);
   const int epb = blockDim.x / (B / V);
   const EoeShared<R> st = stage_eoe<R, J, 1, 0>(m, blockIdx.x * epb, epb, le, nullptr);
+  if (early) pdl_begin();
   if (mine) tl_edge_diag_body<R, V, J>(m, B, bs, ut, ht, d, ph, e, b, st);
 }
 
@@ -464,16 +465,18 @@ __global__ void k_tl_edge_tend(MeshDev<R> m, int B, Base<R> bs, const R *__restr
 }
 
 // k_tl_edge_tend with the edgesOnEdge lists staged in shared memory: one block per epb edges.
+// early: copy the lists before waiting for the previous kernel (g_stable_base).
 template <typename R, typename A, int V, int J>
 __global__ void k_tl_edge_tend_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                                   const R *__restrict__ ht, Diag<R> d, Phys<R> ph, RK<R, A> rk,
-                                  R *tend_u) {
-  pdl_begin();
+                                  R *tend_u, int early) {
+  if (!early) pdl_begin();
   int le, e, b;
   const bool mine = staged_edge(m.nE, B, V, &le, &e, &b);
   const int epb = blockDim.x / (B / V);
   const R *const fields[3] = {bs.pe, bs.u, bs.he};
   const EoeShared<R> st = stage_eoe<R, J, 1, 3>(m, blockIdx.x * epb, epb, le, fields);
+  if (early) pdl_begin();
   if (mine) tl_edge_tend_body<R, A, V, J>(m, B, bs, ut, ht, d, ph, rk, tend_u, e, b, st);
 }
 
@@ -583,13 +586,14 @@ __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
 // staged in shared memory: one block per epb edges.
 template <typename R, typename A, int V, int J>
 __global__ void k_ad_edge_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
-                             AdWork<R> w) {
-  pdl_begin();
+                             AdWork<R> w, int early) {
+  if (!early) pdl_begin();
   int le, e, b;
   const bool mine = staged_edge(m.nE, B, V, &le, &e, &b);
   const int epb = blockDim.x / (B / V);
   const R *const fields[3] = {bs.u, bs.he, bs.pe};
   const EoeShared<R> st = stage_eoe<R, J, 2, 3>(m, blockIdx.x * epb, epb, le, fields);
+  if (early) pdl_begin();
   if (mine) ad_edge_body<R, A, V, J>(m, B, bs, ph, in, sd, w, e, b, st);
 }
 
@@ -853,9 +857,10 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
 // k_ad_final with staged edge lists: the first cell_blocks blocks take the cells (one member
 // group per thread), the others epb edges each with their lists in shared memory.
 template <typename R, typename A, int V, int J>
-__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out, int cell_blocks) {
-  pdl_begin();
+__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out, int cell_blocks,
+                              int early) {
   if ((int)blockIdx.x < cell_blocks) {
+    pdl_begin();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < (long long)m.nC * (B / V)) {
       const EntMember q = ent_member(t, B, V);
@@ -867,7 +872,9 @@ __global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOu
   const int le = threadIdx.x / tpe;
   const int e = ((int)blockIdx.x - cell_blocks) * epb + le;
   const int b = (threadIdx.x - le * tpe) * V;
+  if (!early) pdl_begin();
   const EoeShared<R> st = stage_eoe<R, J, 2, 0>(m, ((int)blockIdx.x - cell_blocks) * epb, epb, le, nullptr);
+  if (early) pdl_begin();
   if (le < epb && e < m.nE) ad_final_edge<R, A, V, J>(m, B, bs, w, out, e, b, st);
 }
 

@@ -497,6 +497,7 @@ static void window_tl_impl(Engine &E, int prec, int B, double *user_u, double *u
     GraphKey key = E.graph_key(7, prec, B, du, dh);
     key.p3 = W.st[prec].mem;
     key.n2 = ((long long)W.nsteps << 20) | W.every;
+    StableBaseScope stable(true);  // the members read only stored stages
     E.run_graph(key, [&]() {
       cuda_check(cudaEventRecord(E.ev_fork, E.stream), "event record");
       cuda_check(cudaStreamWaitEvent(E.side, E.ev_fork, 0), "event wait");
@@ -517,6 +518,7 @@ static void window_tl_impl(Engine &E, int prec, int B, double *user_u, double *u
     GraphKey key = E.graph_key(4, prec, B, du, dh);
     key.p3 = W.st[prec].mem;
     key.n2 = W.nsteps;
+    StableBaseScope stable(true);
     E.run_graph(key, [&]() {
       for (int n = 0; n < W.nsteps; n++)
         for (int k = 0; k < 4; k++)
@@ -599,6 +601,7 @@ static void window_ad_impl(Engine &E, int prec, int B, double *user_u, double *u
     GraphKey key = E.graph_key(5, prec, B, au, ah);
     key.p3 = W.st[prec].mem;
     key.n2 = W.nsteps;
+    StableBaseScope stable(true);
     E.run_graph(key, [&]() {
       tinit();
       for (int n = W.nsteps - 1; n >= 0; n--)
@@ -746,6 +749,7 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
   out.tu_next = mb->pad_u[1]; out.th_next = mb->pad_h[1];
   out.pad_out_u = mb->tk_u[1]; out.pad_out_h = mb->tk_h[1];
   out.wu = w[1]; out.cu = c[1]; out.wh = w[1]; out.ch = c[1];
+  StableBaseScope stable(true);  // the timed kernels write no linearisation point
   auto launch = [&]() {
     using LR = Launch<R, double>;
     switch (which) {
