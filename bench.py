@@ -251,12 +251,12 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
         'tl_edge_tend': eoe + (2 * i + s) * E + 3 * s * E                      # c1,c2,dc; base pv_edge,u,h_edge
                         + B * (s * (3 * E + 2 * C) + (a + 2 * s) * E),         # u,pe,he,ke,h in; RK
         'ad_edge': eoe + s * S + (2 * i + s) * E + 6 * s * E                   # wrev; c1,c2,dv; 6 base fields
-                   + B * s * (E + C + 6 * E),                                  # tu,th in; 6 adjoints out
-        'ad_cell': (i + 6 * i + 6 + s) * C + s * E                             # c_n,es,esg,area; dc
-                   + B * s * (3 * E + 4 * C),                                  # tu,gpn_ad,he_ad in; 4 out
-        'ad_vertex': (3 * i + 3 * s + 3 * i + 3 * i + 3 + 2 * s) * V + s * C + s * E + 2 * s * V
-                     + B * s * (C + 2 * E + 2 * V),                            # pc_ad,pe_ad,gpt_ad in; 2 out
-        'ad_final': (i + 6 * i + 6 * s + s) * C + i * (E + S) + s * S + (4 * i + 2 * s) * E + s * E
+                   + B * s * (E + C + 3 * E),                                  # tu,th in; pe_ad,he_ad,ud out
+        'ad_cell': (i + 6 * i + 6 + s) * C + 2 * s * E                         # c_n,es,esg,area; dc; base u
+                   + B * s * (3 * E + 4 * C),                                  # tu,pe_ad,he_ad in; 4 out
+        'ad_vertex': (3 * i + 3 * s + 3 * i + 3 * i + 3 + 2 * s) * V + s * C + 2 * s * E + 2 * s * V
+                     + B * s * (C + E + 2 * V),                                # pc_ad,pe_ad in; 2 out
+        'ad_final': (i + 6 * i + 6 * s + s) * C + i * (E + S) + s * S + (4 * i + 2 * s) * E + 2 * s * E
                     + B * (s * (2 * C + 2 * V + 2 * E + C) + (a + 2 * s) * (C + E)),
     }
     kb['tl_stage'] = sum(kb[k] for k in ('tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend'))

@@ -276,16 +276,16 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
     case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V)), tuned_block(K_AD_VERTEX)), s, m, B, bs, ph, in, sd, w); break;
     case 3: {
       constexpr int J = BoundsNarrow::e2;
-      constexpr size_t eb = eoe_stage_bytes<R, J, 2, 0>();
+      constexpr size_t eb = eoe_stage_bytes<R, J, 2, 1>();
       const int bk = tuned_block(K_AD_FINAL);
       if (use_staged(m, B, V, eb, bk)) {
         LaunchCfg c = staged_cfg(m.nE, B, V, eb, bk);
         const long long cthreads = (long long)m.nC * (B / V);
         const int cell_blocks = (int)((cthreads + c.block - 1) / c.block);
         c.grid += cell_blocks;
-        launch_k(k_ad_final_st<R, A, V, J>, c, s, m, B, bs, w, out, cell_blocks, (int)g_stable_base);
+        launch_k(k_ad_final_st<R, A, V, J>, c, s, m, B, bs, ph, w, out, cell_blocks, (int)g_stable_base);
       } else {
-        launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), bk), s, m, B, bs, w, out);
+        launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), bk), s, m, B, bs, ph, w, out);
       }
       break;
     }

@@ -568,9 +568,11 @@ __device__ __forceinline__ void ad_edge_body(const MeshDev<R> &m, int B, const B
   stv<V>(w.pe_ad + o, pe_ad);
   stv<V>(w.he_ad + o, he_ad);
   stv<V>(w.ud + o, ud);
-  stv<V>(w.gpn_ad + o, gpn_ad);
-  stv<V>(w.gpt_ad + o, gpt_ad);
-  stv<V>(w.v_ad + o, v_ad);
+  // without seeds the window sweeps leave these null: gradPVn_ad, gradPVt_ad and v_ad are then
+  // re-formed from pv_edge_ad by their readers with these same expressions
+  if (w.gpn_ad) stv<V>(w.gpn_ad + o, gpn_ad);
+  if (w.gpt_ad) stv<V>(w.gpt_ad + o, gpt_ad);
+  if (w.v_ad) stv<V>(w.v_ad + o, v_ad);
 }
 
 template <typename R, typename A, int V, class NB>
@@ -673,7 +675,9 @@ __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
       const size_t oe = (size_t)e * B + q.b;
       const M Te = ldv<V>(in.tu + oe);
       const R dce = ld(m.e_dc, e);
-      pc_ad = pc_ad + (-sg) * (ldv<V>(w.gpn_ad + oe) / dce);
+      const M gpn_ad = w.gpn_ad ? ldv<V>(w.gpn_ad + oe)
+                                : mv_fill<R, V>(R(0)) - ((ph.apvm * ld(bs.u, e)) * ph.dt) * ldv<V>(w.pe_ad + oe);
+      pc_ad = pc_ad + (-sg) * (gpn_ad / dce);
       ke_ad = ke_ad + sg * (Te / dce);
       hd = hd + sg * ((R(GRAVITY) / dce) * Te);
       if (ph.drag) {
@@ -726,7 +730,9 @@ __global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R>
       const R sg = R(m.v_esg[(size_t)k * nV + v]);
       const R dve = ld(m.e_dv, e);
       const size_t oe = (size_t)e * B + q.b;
-      pvv_ad = pvv_ad + sg * (ldv<V>(w.gpt_ad + oe) / dve);
+      const M gpt_ad = w.gpt_ad ? ldv<V>(w.gpt_ad + oe)
+                                : mv_fill<R, V>(R(0)) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * ldv<V>(w.pe_ad + oe);
+      pvv_ad = pvv_ad + sg * (gpt_ad / dve);
       if (ph.visc2 > R(0)) {
         const M ud2 = (ld(m.e_sc2, e) * ph.visc2) * ldv<V>(in.tu + oe);
         vort_ad = vort_ad + (-sg) * (ud2 / dve);
@@ -820,14 +826,20 @@ __device__ __forceinline__ void ad_final_cell(const MeshDev<R> &m, int B, const 
   ad_emit<R, A, V>(out, 0, (size_t)c * B + b, ph_, ld(m.c_area, c));
 }
 
+// l's field 0 is gradPVt of the linearisation point at the neighbours (to re-form v_ad).
 template <typename R, typename A, int V, int NMAX, class L>
-__device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const Base<R> &bs, const AdWork<R> &w,
-                                              const AdOut<R, A> &out, int e, int b, const L &l) {
+__device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
+                                              const AdWork<R> &w, const AdOut<R, A> &out, int e, int b,
+                                              const L &l) {
   using M = Mv<R, V>;
   const int n = ld(m.e_n, e);
   M pu = ldv<V>(w.ud + (size_t)e * B + b);
-  MPSW_SLOTS(j, NMAX, n)
-    pu = pu + l.wr(j) * ldv<V>(w.v_ad + (size_t)l.nb(j) * B + b);
+  MPSW_SLOTS(j, NMAX, n) {
+    const size_t on = (size_t)l.nb(j) * B + b;
+    const M v_ad = w.v_ad ? ldv<V>(w.v_ad + on)
+                          : mv_fill<R, V>(R(0)) - ((ph.apvm * ph.dt) * l.f(0, j)) * ldv<V>(w.pe_ad + on);
+    pu = pu + l.wr(j) * v_ad;
+  }
   const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
   const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
   const R kc = (((R(0.25) * dc) * dv) * R(2)) * ld(bs.u, e);
@@ -841,7 +853,7 @@ __device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const 
 }
 
 template <typename R, typename A, int V, class NB>
-__global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out) {
+__global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWork<R> w, AdOut<R, A> out) {
   const long long tc = (long long)m.nC * (B / V);
   MPSW_GRID_LOOP(t, tc + (long long)m.nE * (B / V)) {
     if (t < tc) {
@@ -849,7 +861,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
       ad_final_cell<R, A, V, NB::c>(m, B, w, out, q.ent, q.b);
     } else {
       const EntMember q = ent_member(t - tc, B, V);
-      ad_final_edge<R, A, V, NB::e2>(m, B, bs, w, out, q.ent, q.b, eoe_global(m, q.ent));
+      ad_final_edge<R, A, V, NB::e2>(m, B, bs, ph, w, out, q.ent, q.b, eoe_global(m, q.ent, bs.gpt));
     }
   }
 }
@@ -857,8 +869,8 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R
 // k_ad_final with staged edge lists: the first cell_blocks blocks take the cells (one member
 // group per thread), the others epb edges each with their lists in shared memory.
 template <typename R, typename A, int V, int J>
-__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOut<R, A> out, int cell_blocks,
-                              int early) {
+__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWork<R> w, AdOut<R, A> out,
+                              int cell_blocks, int early) {
   if ((int)blockIdx.x < cell_blocks) {
     pdl_begin();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -873,9 +885,10 @@ __global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, AdWork<R> w, AdOu
   const int e = ((int)blockIdx.x - cell_blocks) * epb + le;
   const int b = (threadIdx.x - le * tpe) * V;
   if (!early) pdl_begin();
-  const EoeShared<R> st = stage_eoe<R, J, 2, 0>(m, ((int)blockIdx.x - cell_blocks) * epb, epb, le, nullptr);
+  const R *const fields[1] = {bs.gpt};
+  const EoeShared<R> st = stage_eoe<R, J, 2, 1>(m, ((int)blockIdx.x - cell_blocks) * epb, epb, le, fields);
   if (early) pdl_begin();
-  if (le < epb && e < m.nE) ad_final_edge<R, A, V, J>(m, B, bs, w, out, e, b, st);
+  if (le < epb && e < m.nE) ad_final_edge<R, A, V, J>(m, B, bs, ph, w, out, e, b, st);
 }
 
 }  // namespace mpsw

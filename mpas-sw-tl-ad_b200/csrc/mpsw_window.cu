@@ -79,7 +79,8 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   }
   AdWork<R> &w = mb->w;
   w.pe_ad = walloc<R>(M, Ed, s); w.he_ad = walloc<R>(M, Ed, s); w.ud = walloc<R>(M, Ed, s);
-  w.gpn_ad = walloc<R>(M, Ed, s); w.gpt_ad = walloc<R>(M, Ed, s); w.v_ad = walloc<R>(M, Ed, s);
+  // gradPVn_ad, gradPVt_ad, v_ad: re-formed from pv_edge_ad by their readers (no seeds here)
+  w.gpn_ad = nullptr; w.gpt_ad = nullptr; w.v_ad = nullptr;
   w.du_ad = walloc<R>(M, Ed, s);
   w.pc_ad = walloc<R>(M, C, s); w.ke_ad = walloc<R>(M, C, s); w.div_ad = walloc<R>(M, C, s);
   w.hd = walloc<R>(M, C, s); w.dd_ad = walloc<R>(M, C, s);
