@@ -198,6 +198,11 @@ void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const 
                                     rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1], rk.t_in[2]},
                                 tuned_v(K_TL_CELL));
   const int bk = tuned_block(K_TL_CELL);
+  if (use_staged(m, B, v, cell_stage_bytes<R>(), bk)) {
+    MPSW_VDISPATCH(v, launch_k(k_tl_cell_st<R, A, VV>, staged_cfg(m.nC, B, VV, cell_stage_bytes<R>(), bk), s, m, B,
+                               bs, ut, ht, d, rk, tend_h, (int)g_stable_base));
+    return;
+  }
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_cell<R, A, VV, NB>, launch_cfg((long long)(m.nC) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, d, rk, tend_h)));
 }
 template <typename R, typename A>

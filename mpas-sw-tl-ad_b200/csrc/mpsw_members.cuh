@@ -347,6 +347,96 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_tl_cell(MeshDev
   }
 }
 
+// Shared-memory bytes per cell of tl_cell_st's stage: 6 slots of 4 indices and 7 coefficients.
+template <typename R>
+__host__ __device__ constexpr size_t cell_stage_bytes() {
+  return (size_t)BoundsNarrow::c * (4 * sizeof(int) + 7 * sizeof(R));
+}
+
+// k_tl_cell with each block's cell lists staged in shared memory (meshes with at most 6
+// edgesOnCell): per slot the edge (reference scatter order) and its sign, the cell across it,
+// dvEdge, the linearisation point's h_edge and u there, the edgesOnCell edge with its two ke
+// coefficients, and the vertex with its kite.  The member loads then take their addresses from
+// shared memory, and h at the cell itself is loaded once (h_edge is the same sum in either
+// order).  early: copy the lists before waiting for the previous kernel.
+template <typename R, typename A, int V>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
+    k_tl_cell_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut, const R *__restrict__ ht, Diag<R> d,
+                 RK<R, A> rk, R *tend_h, int early) {
+  using M = Mv<R, V>;
+  constexpr int S = BoundsNarrow::c;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (!early) pdl_begin();
+  const int nC = m.nC, tpe = B / V, cpb = blockDim.x / tpe;
+  const int c0 = blockIdx.x * cpb;
+  R *sr = reinterpret_cast<R *>(smem_raw);  // [7][S][cpb]
+  int *si = reinterpret_cast<int *>(sr + (size_t)7 * S * cpb);  // [4][S][cpb]
+  const size_t SC = (size_t)S * cpb;
+  for (int i = threadIdx.x; i < S * cpb; i += blockDim.x) {
+    const int k = i / cpb, lc = i - k * cpb, c = c0 + lc;
+    int e = 0, nb = 0, eo = 0, v = 0;
+    R sg = R(0), dve = R(0), heb = R(0), ub = R(0), k1 = R(0), k2 = R(0), kt = R(0);
+    if (c < nC && k < ld(m.c_n, c)) {
+      e = ld(m.c_es, (size_t)k * nC + c);
+      sg = R(m.c_esg[(size_t)k * nC + c]);
+      const int c1 = ld(m.e_c1, e);
+      nb = c1 == c ? ld(m.e_c2, e) : c1;
+      dve = ld(m.e_dv, e);
+      heb = ld(bs.he, e);
+      ub = ld(bs.u, e);
+      eo = ld(m.c_eoc, (size_t)k * nC + c);
+      k1 = (R(0.25) * ld(m.e_dc, eo)) * ld(m.e_dv, eo);
+      k2 = R(2) * ld(bs.u, eo);
+      v = ld(m.c_vs, (size_t)k * nC + c);
+      kt = ld(m.c_vk, (size_t)k * nC + c);
+    }
+    sr[0 * SC + i] = sg; sr[1 * SC + i] = dve; sr[2 * SC + i] = heb; sr[3 * SC + i] = ub;
+    sr[4 * SC + i] = k1; sr[5 * SC + i] = k2; sr[6 * SC + i] = kt;
+    si[0 * SC + i] = e; si[1 * SC + i] = nb; si[2 * SC + i] = eo; si[3 * SC + i] = v;
+  }
+  __syncthreads();
+  if (early) pdl_begin();
+  const int lc = threadIdx.x / tpe, c = c0 + lc;
+  if (lc >= cpb || c >= nC) return;
+  const int b = (threadIdx.x - lc * tpe) * V;
+  const int n = ld(m.c_n, c);
+  const M htc = ldv<V>(ht + (size_t)c * B + b);
+  M div = mv_fill<R, V>(R(0)), th = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(k, S, n) {
+    const int i = k * cpb + lc;
+    const R s = sr[0 * SC + i], dve = sr[1 * SC + i];
+    const M ue = ldv<V>(ut + (size_t)si[0 * SC + i] * B + b);
+    div = div + s * (ue * dve);
+    const M het = R(0.5) * (htc + ldv<V>(ht + (size_t)si[1 * SC + i] * B + b));
+    const M flux = (ue * dve) * sr[2 * SC + i] + (sr[3 * SC + i] * dve) * het;
+    th = th + (-s) * flux;
+  }
+  const R area = ld(m.c_area, c);
+  div = div * (R(1) / area);
+  M ke = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(k, S, n) {
+    const int i = k * cpb + lc;
+    ke = ke + sr[4 * SC + i] * (sr[5 * SC + i] * ldv<V>(ut + (size_t)si[2 * SC + i] * B + b));
+  }
+  ke = ke / area;
+  M pc = mv_fill<R, V>(R(0)), vc = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(k, S, n) {
+    const int i = k * cpb + lc;
+    const int v = si[3 * SC + i];
+    const R kt = sr[6 * SC + i];
+    pc = pc + (kt * ldv<V>(d.pvv + (size_t)v * B + b)) / area;
+    if (d.vc) vc = vc + (kt * ldv<V>(d.vort + (size_t)v * B + b)) / area;
+  }
+  th = th / area;
+  const size_t o = (size_t)c * B + b;
+  stv<V>(d.div + o, div);
+  stv<V>(d.ke + o, ke);
+  stv<V>(d.pc + o, pc);
+  if (d.vc) stv<V>(d.vc + o, vc);
+  if (tend_h) stv<V>(tend_h + o, th);
+  rk_members<R, A, V>(rk, o, th);
+}
+
 // :319-329, :364-393, :425-445, h_edge_tl :117-126, delsq_u_tl :638-652.  Body for edge e,
 // members b .. b+V-1; l is the edge's edgesOnEdge list.
 template <typename R, int V, int NMAX, class L>
