@@ -791,6 +791,80 @@ __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
   }
 }
 
+// Shared-memory bytes per cell of ad_cell_st's stage: 6 slots of an edge index and 6 coefficients.
+template <typename R>
+__host__ __device__ constexpr size_t ad_cell_stage_bytes() {
+  return (size_t)BoundsNarrow::c * (sizeof(int) + 6 * sizeof(R));
+}
+
+// k_ad_cell with each block's cell lists staged in shared memory (meshes with at most 6
+// edgesOnCell): per slot the edge (reference scatter order), its sign, dcEdge and the scalar
+// coefficients of the slot's terms (gradPVn, gravity, drag, del2), computed with the same
+// operations as k_ad_cell.  early: copy the lists before waiting for the previous kernel.
+template <typename R, typename A, int V>
+__global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd, AdWork<R> w,
+                             int early) {
+  using M = Mv<R, V>;
+  constexpr int S = BoundsNarrow::c;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (!early) pdl_begin();
+  const int nC = m.nC, tpe = B / V, cpb = blockDim.x / tpe;
+  const int c0 = blockIdx.x * cpb;
+  R *sr = reinterpret_cast<R *>(smem_raw);                      // [6][S][cpb]
+  int *se = reinterpret_cast<int *>(sr + (size_t)6 * S * cpb);  // [S][cpb]
+  const size_t SC = (size_t)S * cpb;
+  for (int i = threadIdx.x; i < S * cpb; i += blockDim.x) {
+    const int k = i / cpb, lc = i - k * cpb, c = c0 + lc;
+    int e = 0;
+    R sg = R(0), dce = R(1), gq = R(0), gg = R(0), kd = R(0), k2 = R(0);
+    if (c < nC && k < ld(m.c_n, c)) {
+      e = ld(m.c_es, (size_t)k * nC + c);
+      sg = R(m.c_esg[(size_t)k * nC + c]);
+      dce = ld(m.e_dc, e);
+      gq = (ph.apvm * ld(bs.u, e)) * ph.dt;
+      gg = R(GRAVITY) / dce;
+      if (ph.drag) {
+        const R sq = sqrt(R(2) * (R(0.5) * (ld(bs.ke, ld(m.e_c1, e)) + ld(bs.ke, ld(m.e_c2, e)))));
+        kd = -(((((R(0.5) * R(1.0e-3)) * ld(bs.u, e)) * R(2)) / sq) / ld(bs.he, e));
+      }
+      if (ph.visc2 > R(0)) k2 = ld(m.e_sc2, e) * ph.visc2;
+    }
+    sr[0 * SC + i] = sg; sr[1 * SC + i] = dce; sr[2 * SC + i] = gq; sr[3 * SC + i] = gg;
+    sr[4 * SC + i] = kd; sr[5 * SC + i] = k2;
+    se[i] = e;
+  }
+  __syncthreads();
+  if (early) pdl_begin();
+  const int lc = threadIdx.x / tpe, c = c0 + lc;
+  if (lc >= cpb || c >= nC) return;
+  const int b = (threadIdx.x - lc * tpe) * V;
+  const int n = ld(m.c_n, c);
+  M pc_ad = mv_fill<R, V>(sd.pc ? sd.pc[c] : R(0));
+  M ke_ad = mv_fill<R, V>(sd.ke ? sd.ke[c] : R(0));
+  M div_ad = mv_fill<R, V>(sd.div ? sd.div[c] : R(0));
+  M hd = mv_fill<R, V>(R(0));
+  MPSW_SLOTS(k, S, n) {
+    const int i = k * cpb + lc;
+    const size_t oe = (size_t)se[i] * B + b;
+    const R sg = sr[0 * SC + i], dce = sr[1 * SC + i];
+    const M Te = ldv<V>(in.tu + oe);
+    const M gpn_ad = w.gpn_ad ? ldv<V>(w.gpn_ad + oe) : mv_fill<R, V>(R(0)) - sr[2 * SC + i] * ldv<V>(w.pe_ad + oe);
+    pc_ad = pc_ad + (-sg) * (gpn_ad / dce);
+    ke_ad = ke_ad + sg * (Te / dce);
+    hd = hd + sg * (sr[3 * SC + i] * Te);
+    if (ph.drag) ke_ad = ke_ad + R(0.5) * (sr[4 * SC + i] * Te);
+    if (ph.visc2 > R(0)) div_ad = div_ad + (-sg) * ((sr[5 * SC + i] * Te) / dce);
+    if (ph.visc4 > R(0)) div_ad = div_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dce);
+    hd = hd + R(0.5) * ldv<V>(w.he_ad + oe);
+  }
+  const R area = ld(m.c_area, c);
+  const size_t o = (size_t)c * B + b;
+  stv<V>(w.pc_ad + o, pc_ad);
+  stv<V>(w.ke_ad + o, ke_ad / area);
+  stv<V>(w.div_ad + o, div_ad * (R(1) / area));
+  stv<V>(w.hd + o, hd);
+}
+
 // Vertex stage: pv_cell -> pv_vertex (:215-229), pv_edge -> pv_vertex (:244-252),
 // gradPVt -> pv_vertex (:254-262), del2/del4 vorticity adjoints, pv_vertex -> h_vertex and
 // vorticity (:268-284), vorticity -> circulation (:343-349).
