@@ -93,7 +93,8 @@ __device__ __forceinline__ EntMember ent_member(long long t, int B, int V) {
 // RK4 bookkeeping of V members (src/mpas_sw_module.f90:590-611)
 template <typename R, typename A, int V>
 __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const Mv<R, V> &t) {
-  if (rk.next) {
+  const bool last = rk.t_in[0] != nullptr;  // the stage that sums the stored tendencies
+  if (rk.next && !last) {
     const Mv<A, V> x0 = ldv<V>(rk.x0 + o);
     Mv<R, V> n;
 #pragma unroll
@@ -114,6 +115,7 @@ __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const M
 #pragma unroll
     for (int i = 0; i < V; i++) a.x[i] = a.x[i] + rk.w * A(t.x[i]);
     stv<V>(rk.acc_out + o, a);
+    if (rk.next) stv<V>(rk.next + o, mv_cast<V, R>(a));  // the next step's rounded stage-1 input
   } else if (rk.acc_out) {
     Mv<A, V> a = ldv<V>(rk.acc_in + o);
 #pragma unroll

@@ -433,30 +433,41 @@ void Engine::window_ensure() {
 }
 
 // Member work of tangent-linear stage k about the linearisation point bs.
+//
+// Stage 1 reads the FP64 member state directly when R is double; otherwise its FP32 rounding in
+// pu[1] / ph[1], made here when `round_in` (the first step of a sweep, or every step where the
+// previous one did not leave it: per-step graphs, test case 1's frozen wind) and otherwise
+// written by the previous step's stage 4 as it formed the new state.  pu[1] / ph[1] are free
+// then: stage 2 overwrites them after stage 1, stage 4 writes them after stage 3 read them.
 template <typename R>
 static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, MemberBufs<R> *mb,
                             const Phys<R> &ph, const double w[4], const double c[4], int k, const Base<R> &bs,
-                            cudaStream_t st) {
+                            cudaStream_t st, bool round_in) {
   Window &W = E.win;
   const MeshDev<R> &m = mesh_for<R>(E);
   const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
   const R *hti = k == 0 ? nullptr : mb->ph[k - 1];
-  // stage 1 reads the FP64 member state directly when R is double; otherwise round it
+  constexpr bool f64 = std::is_same<R, double>::value;
+  const bool hand_on = !f64 && !ph.tc1;  // stage 4 leaves the next step's rounded input
   if (k == 0) {
-    if constexpr (std::is_same<R, double>::value) {
+    if constexpr (f64) {
       uti = du;
       hti = dh;
     } else {
-      convert_d2f((long long)E.nE * B, du, mb->pu[2], st);
-      convert_d2f((long long)E.nC * B, dh, mb->ph[2], st);
-      uti = mb->pu[2];
-      hti = mb->ph[2];
+      if (round_in || ph.tc1) {
+        convert_d2f((long long)E.nE * B, du, mb->pu[1], st);
+        convert_d2f((long long)E.nC * B, dh, mb->ph[1], st);
+      }
+      uti = mb->pu[1];
+      hti = mb->ph[1];
     }
   }
   // stages 1-3 keep their tendencies; stage 4 sums them into the FP64 members (deferred RK4
   // accumulation, the same FP64 additions as accumulating stage by stage)
-  RK<R, double> rut{du, nullptr, k == 3 ? du : nullptr, k < 3 ? mb->pu[k] : nullptr, c[k], w[k], R(0), ph.tc1};
-  RK<R, double> rht{dh, nullptr, k == 3 ? dh : nullptr, k < 3 ? mb->ph[k] : nullptr, c[k], w[k], R(0), 0};
+  R *nu = k < 3 ? mb->pu[k] : (hand_on ? mb->pu[1] : nullptr);
+  R *nh = k < 3 ? mb->ph[k] : (hand_on ? mb->ph[1] : nullptr);
+  RK<R, double> rut{du, nullptr, k == 3 ? du : nullptr, nu, c[k], w[k], R(0), ph.tc1};
+  RK<R, double> rht{dh, nullptr, k == 3 ? dh : nullptr, nh, c[k], w[k], R(0), 0};
   if (k < 3) {
     rut.t_out = mb->tk_u[k];
     rht.t_out = mb->tk_h[k];
@@ -467,7 +478,6 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
       rut.wt[j] = rht.wt[j] = w[j];
     }
   }
-  // stage 3 writes pu[2], which stage 1 used as its rounded input: stage 1 is done by then
   Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, st);
   Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, st);
   Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, st);
@@ -508,7 +518,7 @@ static void window_tl_impl(Engine &E, int prec, int B, double *user_u, double *u
         cuda_check(cudaEventRecord(E.ev_step, E.stream), "event record");
         cuda_check(cudaStreamWaitEvent(E.side, E.ev_step, 0), "event wait");
         for (int k = 0; k < 4; k++)
-          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k), E.side);
+          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k), E.side, n == 0);
       }
       cuda_check(cudaEventRecord(E.ev_join, E.side), "event record");
       cuda_check(cudaStreamWaitEvent(E.stream, E.ev_join, 0), "event wait");
@@ -523,7 +533,7 @@ static void window_tl_impl(Engine &E, int prec, int B, double *user_u, double *u
     E.run_graph(key, [&]() {
       for (int n = 0; n < W.nsteps; n++)
         for (int k = 0; k < 4; k++)
-          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k), E.stream);
+          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, stored_base<R>(W, prec, n, k), E.stream, n == 0);
     });
   } else {
     E.window_ensure();
@@ -534,7 +544,9 @@ static void window_tl_impl(Engine &E, int prec, int B, double *user_u, double *u
     const GraphKey key = E.graph_key(2, prec, B, du, dh);
     for (int n = 0; n < W.nsteps; n++)
       E.run_graph(key, [&]() {
-        traj_step(E, true, prec, [&](int k) { tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, base_for<R>(W, k), E.stream); });
+        traj_step(E, true, prec, [&](int k) {
+          tl_member_stage<R>(E, prec, B, du, dh, mb, ph, w, c, k, base_for<R>(W, k), E.stream, true);
+        });
       });
   }
   members_copy(E, B, user_u, user_h, du, dh);
