@@ -468,7 +468,8 @@ def run_mpsw(a, rank, world):
             'batched_vs_plain': (value / world / plain) if plain else None,
             'rel_err_fp32_vs_fp64': rel_err,
             'e2e': {'value': e2e_val, 'unit': UNIT, 'h2d_bytes_per_step': int(du_host.numel() * 8 + dh_host.numel() * 8),
-                    'd2h_bytes_per_step': int(out_u.numel() * 8 + out_h.numel() * 8)},
+                    'd2h_bytes_per_step': int(out_u.numel() * 8 + out_h.numel() * 8),
+                    'step_ms': [round(t, 3) for t in te]},
             'roofline': roof,
             'cpu_baseline': cpu,
             'clocks': clocks,
