@@ -175,6 +175,7 @@ struct EoeGlobal {
   __device__ R w(int j) const { return ld(wv, (size_t)j * nE + e); }
   __device__ R wr(int j) const { return ld(wrv, (size_t)j * nE + e); }
   __device__ R f(int k, int j) const { return ld(fld[k], nb(j)); }
+  static constexpr bool kPadded = false;  // slots at or past nEdgesOnEdge must not be read
 };
 template <typename R>
 __device__ __forceinline__ EoeGlobal<R> eoe_global(const MeshDev<R> &m, int e, const R *f0 = nullptr,
@@ -201,6 +202,9 @@ struct EoeShared {
   __device__ R w(int j) const { return sw[at(j)]; }
   __device__ R wr(int j) const { return swr[at(j)]; }
   __device__ R f(int k, int j) const { return sf[(size_t)k * J * epb + at(j)]; }
+  // Slots at or past nEdgesOnEdge hold neighbour 0 with zero weights and fields: every term of
+  // such a slot is an exact zero, so a body may run all J slots without a bound check.
+  static constexpr bool kPadded = true;
 };
 
 // Shared-memory bytes per edge of a stage with HW weights arrays (0-2) and NF fields.
@@ -360,7 +364,9 @@ __host__ __device__ constexpr size_t cell_stage_bytes() {
 // dvEdge, the linearisation point's h_edge and u there, the edgesOnCell edge with its two ke
 // coefficients, and the vertex with its kite.  The member loads then take their addresses from
 // shared memory, and h at the cell itself is loaded once (h_edge is the same sum in either
-// order).  early: copy the lists before waiting for the previous kernel.
+// order).  Slots past the cell's edge count hold index 0 with zero coefficients, so every term
+// there is an exact zero and all 6 slots run without a bound check.  early: copy the lists
+// before waiting for the previous kernel.
 template <typename R, typename A, int V>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
     k_tl_cell_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut, const R *__restrict__ ht, Diag<R> d,
@@ -401,10 +407,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
   const int lc = threadIdx.x / tpe, c = c0 + lc;
   if (lc >= cpb || c >= nC) return;
   const int b = (threadIdx.x - lc * tpe) * V;
-  const int n = ld(m.c_n, c);
   const M htc = ldv<V>(ht + (size_t)c * B + b);
   M div = mv_fill<R, V>(R(0)), th = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(k, S, n) {
+  MPSW_SLOTS(k, S, S) {
     const int i = k * cpb + lc;
     const R s = sr[0 * SC + i], dve = sr[1 * SC + i];
     const M ue = ldv<V>(ut + (size_t)si[0 * SC + i] * B + b);
@@ -416,13 +421,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
   const R area = ld(m.c_area, c);
   div = div * (R(1) / area);
   M ke = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(k, S, n) {
+  MPSW_SLOTS(k, S, S) {
     const int i = k * cpb + lc;
     ke = ke + sr[4 * SC + i] * (sr[5 * SC + i] * ldv<V>(ut + (size_t)si[2 * SC + i] * B + b));
   }
   ke = ke / area;
   M pc = mv_fill<R, V>(R(0)), vc = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(k, S, n) {
+  MPSW_SLOTS(k, S, S) {
     const int i = k * cpb + lc;
     const int v = si[3 * SC + i];
     const R kt = sr[6 * SC + i];
@@ -448,7 +453,7 @@ __device__ __forceinline__ void tl_edge_diag_body(const MeshDev<R> &m, int B, co
   using M = Mv<R, V>;
   const int n = ld(m.e_n, e);
   M vt = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(j, NMAX, n)
+  MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n)
     vt = vt + l.w(j) * ldv<V>(ut + (size_t)l.nb(j) * B + b);
   const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
   const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
@@ -504,7 +509,7 @@ __device__ __forceinline__ void tl_edge_tend_body(const MeshDev<R> &m, int B, co
   const M pet_e = ldv<V>(d.pe + (size_t)e * B + b);
   const R pe_e = ld(bs.pe, e);
   M qt = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(j, NMAX, n) {
+  MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n) {
     const int eoe = l.nb(j);
     const R w = l.w(j);
     const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + b));
@@ -624,7 +629,7 @@ __device__ __forceinline__ void ad_edge_body(const MeshDev<R> &m, int B, const B
   const M Te = ldv<V>(in.tu + (size_t)e * B + b);
   const R ue = ld(bs.u, e), hee = ld(bs.he, e), pee = ld(bs.pe, e);
   M pe_ad = mv_fill<R, V>(R(0)), he_ad = mv_fill<R, V>(R(0)), ud = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(j, NMAX, n) {
+  MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n) {
     const int nb = l.nb(j);
     const R wj = l.w(j);
     const R wr = l.wr(j);
@@ -1000,7 +1005,7 @@ __device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const 
   using M = Mv<R, V>;
   const int n = ld(m.e_n, e);
   M pu = ldv<V>(w.ud + (size_t)e * B + b);
-  MPSW_SLOTS(j, NMAX, n) {
+  MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n) {
     const size_t on = (size_t)l.nb(j) * B + b;
     const M v_ad = w.v_ad ? ldv<V>(w.v_ad + on)
                           : mv_fill<R, V>(R(0)) - ((ph.apvm * ph.dt) * l.f(0, j)) * ldv<V>(w.pe_ad + on);
