@@ -54,6 +54,12 @@ struct BoundsAny {
   _Pragma("unroll") for (int j = 0; j < ((NMAX) > 0 ? (NMAX) : (n)); j++) \
     if ((NMAX) == 0 || j < (n))
 
+// The device mesh pads every list past its entity's count with index 0 and zero weights, signs
+// and kites (MAXE2 slots for edgesOnEdge, MAXE for the cell lists).  A term whose coefficient
+// is one of those padded values is an exact zero there, so such a loop may run all NMAX slots of
+// a narrow mesh without a bound check: MPSW_PADDED(j, NMAX, n).
+#define MPSW_PADDED(j, NMAX, n) MPSW_SLOTS(j, NMAX, ((NMAX) > 0 ? (NMAX) : (n)))
+
 
 // ----------------------------------------------------------------------------------------
 // Forward: sw_compute_solve_diagnostics (src/mpas_sw_dyncore.f90:1-361) split by entity.
@@ -93,7 +99,7 @@ __global__ void k_fwd_vertex(MeshDev<R> m, const R *__restrict__ u, const R *__r
 // tendency (:468-482) with its RK update.
 // c_nb[k][c] is the cell across edge k of the cell (its h_edge sums this cell's h and that
 // cell's, in either order: the same value)
-template <typename R, typename A>
+template <typename R, typename A, int NC>
 __global__ void k_fwd_cell(MeshDev<R> m, const int *__restrict__ c_nb, const R *__restrict__ u,
                            const R *__restrict__ h, R off, Diag<R> d, RK<R, A> rk, R *tend_h) {
   const int nC = m.nC;
@@ -102,7 +108,7 @@ __global__ void k_fwd_cell(MeshDev<R> m, const int *__restrict__ c_nb, const R *
     const int n = ld(m.c_n, c);
     const R hc = ld(h, c) + off;
     R div = R(0), th = R(0);
-    for (int k = 0; k < n; k++) {
+    MPSW_PADDED(k, NC, n) {
       const int e = ld(m.c_es, (size_t)k * nC + c);
       const R s = R(m.c_esg[(size_t)k * nC + c]);
       const R ue = ld(u, e), dve = ld(m.e_dv, e);
@@ -120,7 +126,7 @@ __global__ void k_fwd_cell(MeshDev<R> m, const int *__restrict__ c_nb, const R *
     }
     ke = ke / area;
     R pc = R(0), vc = R(0);
-    for (int k = 0; k < n; k++) {
+    MPSW_PADDED(k, NC, n) {
       const int v = ld(m.c_vs, (size_t)k * nC + c);
       const R kt = ld(m.c_vk, (size_t)k * nC + c);
       pc = pc + (kt * d.pvv[v]) / area;
@@ -139,7 +145,7 @@ __global__ void k_fwd_cell(MeshDev<R> m, const int *__restrict__ c_nb, const R *
 
 // tangential velocity (:259-267), gradPVt (:296-301), pv_edge with both APVM terms
 // (:305-320, :344-359), h_edge (:95-105) and, for del4, delsq_u (:539-551).
-template <typename R>
+template <typename R, int NE>
 __global__ void k_fwd_edge_diag(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ h, R off,
                                 Diag<R> d, Phys<R> ph) {
   const int nE = m.nE;
@@ -147,7 +153,7 @@ __global__ void k_fwd_edge_diag(MeshDev<R> m, const R *__restrict__ u, const R *
     const int e = (int)t;
     const int n = ld(m.e_n, e);
     R v = R(0);
-    for (int j = 0; j < n; j++)
+    MPSW_PADDED(j, NE, n)
       v = v + ld(m.e_w, (size_t)j * nE + e) * ld(u, ld(m.e_eoe, (size_t)j * nE + e));
     const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
     const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
@@ -168,7 +174,7 @@ __global__ void k_fwd_edge_diag(MeshDev<R> m, const R *__restrict__ u, const R *
 }
 
 // Normal-velocity tendency (src/mpas_sw_dyncore.f90:485-637) and its RK update.
-template <typename R, typename A>
+template <typename R, typename A, int NE>
 __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ h, R off,
                                 Diag<R> d, Phys<R> ph, RK<R, A> rk, R *tend_u) {
   const int nE = m.nE;
@@ -177,7 +183,7 @@ __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *
     const int n = ld(m.e_n, e);
     const R pee = d.pe[e];
     R q = R(0);
-    for (int j = 0; j < n; j++) {
+    MPSW_PADDED(j, NE, n) {
       const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
       const R wpv = R(0.5) * (pee + d.pe[eoe]);
       q = q + ((ld(m.e_w, (size_t)j * nE + e) * ld(u, eoe)) * wpv) * d.he[eoe];

@@ -148,7 +148,7 @@ template <typename R, typename A>
 void Launch<R, A>::fwd_cell(const MeshDev<R> &m, const int *c_nb, const R *u, const R *h, R off,
                             const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
-  launch_k(k_fwd_cell<R, A>, launch_cfg(m.nC), s, m, c_nb, u, h, off, d, rk, tend_h);
+  MPSW_BDISPATCH(m, launch_k(k_fwd_cell<R, A, NB::c>, launch_cfg(m.nC), s, m, c_nb, u, h, off, d, rk, tend_h));
 }
 template <typename R, typename A>
 void Launch<R, A>::fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
@@ -156,7 +156,7 @@ void Launch<R, A>::fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R 
   g_launches++;
   Diag<R> dd = d;
   if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
-  launch_k(k_fwd_edge_diag<R>, launch_cfg(m.nE), s, m, u, h, off, dd, ph);
+  MPSW_BDISPATCH(m, launch_k(k_fwd_edge_diag<R, NB::e2>, launch_cfg(m.nE), s, m, u, h, off, dd, ph));
 }
 template <typename R, typename A>
 void Launch<R, A>::del4_vc(const MeshDev<R> &m, int B, const R *dsq_u, R *dsq_vort, R *dsq_div,
@@ -169,7 +169,7 @@ template <typename R, typename A>
 void Launch<R, A>::fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                                  const Phys<R> &ph, const RK<R, A> &rk, R *tend_u, cudaStream_t s) {
   g_launches++;
-  launch_k(k_fwd_edge_tend<R, A>, launch_cfg(m.nE), s, m, u, h, off, d, ph, rk, tend_u);
+  MPSW_BDISPATCH(m, launch_k(k_fwd_edge_tend<R, A, NB::e2>, launch_cfg(m.nE), s, m, u, h, off, d, ph, rk, tend_u));
 }
 template <typename R, typename A>
 void Launch<R, A>::tend_h(const MeshDev<R> &m, const R *u, const R *he, R *out, cudaStream_t s) {
