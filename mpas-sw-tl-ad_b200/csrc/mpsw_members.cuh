@@ -807,7 +807,9 @@ __host__ __device__ constexpr size_t ad_cell_stage_bytes() {
 // k_ad_cell with each block's cell lists staged in shared memory (meshes with at most 6
 // edgesOnCell): per slot the edge (reference scatter order), its sign, dcEdge and the scalar
 // coefficients of the slot's terms (gradPVn, gravity, drag, del2), computed with the same
-// operations as k_ad_cell.  early: copy the lists before waiting for the previous kernel.
+// operations as k_ad_cell.  Slots past the cell's edge count hold edge 0 with sign 0, dcEdge 1
+// and zero coefficients, so every term there is an exact zero and all 6 slots run without a
+// bound check.  early: copy the lists before waiting for the previous kernel.
 template <typename R, typename A, int V>
 __global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd, AdWork<R> w,
                              int early) {
@@ -845,15 +847,15 @@ __global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R
   const int lc = threadIdx.x / tpe, c = c0 + lc;
   if (lc >= cpb || c >= nC) return;
   const int b = (threadIdx.x - lc * tpe) * V;
-  const int n = ld(m.c_n, c);
   M pc_ad = mv_fill<R, V>(sd.pc ? sd.pc[c] : R(0));
   M ke_ad = mv_fill<R, V>(sd.ke ? sd.ke[c] : R(0));
   M div_ad = mv_fill<R, V>(sd.div ? sd.div[c] : R(0));
   M hd = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(k, S, n) {
+  MPSW_SLOTS(k, S, S) {
     const int i = k * cpb + lc;
     const size_t oe = (size_t)se[i] * B + b;
     const R sg = sr[0 * SC + i], dce = sr[1 * SC + i];
+    const R half = R(0.5) * (sg * sg);  // 0.5 (sg is +-1), or 0 in a padded slot
     const M Te = ldv<V>(in.tu + oe);
     const M gpn_ad = w.gpn_ad ? ldv<V>(w.gpn_ad + oe) : mv_fill<R, V>(R(0)) - sr[2 * SC + i] * ldv<V>(w.pe_ad + oe);
     pc_ad = pc_ad + (-sg) * (gpn_ad / dce);
@@ -862,7 +864,7 @@ __global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R
     if (ph.drag) ke_ad = ke_ad + R(0.5) * (sr[4 * SC + i] * Te);
     if (ph.visc2 > R(0)) div_ad = div_ad + (-sg) * ((sr[5 * SC + i] * Te) / dce);
     if (ph.visc4 > R(0)) div_ad = div_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dce);
-    hd = hd + R(0.5) * ldv<V>(w.he_ad + oe);
+    hd = hd + half * ldv<V>(w.he_ad + oe);
   }
   const R area = ld(m.c_area, c);
   const size_t o = (size_t)c * B + b;
@@ -992,7 +994,7 @@ __device__ __forceinline__ void ad_final_cell(const MeshDev<R> &m, int B, const 
   const int nC = m.nC;
   const int n = ld(m.c_n, c);
   M ph_ = ldv<V>(w.hd + (size_t)c * B + b);
-  MPSW_SLOTS(k, NMAX, n)
+  MPSW_PADDED(k, NMAX, n)
     ph_ = ph_ + ld(m.c_vk, (size_t)k * nC + c) * ldv<V>(w.hv_ad + (size_t)ld(m.c_vs, (size_t)k * nC + c) * B + b);
   ad_emit<R, A, V>(out, 0, (size_t)c * B + b, ph_, ld(m.c_area, c));
 }
