@@ -126,6 +126,8 @@ const ScalarSpec kScalars[] = {
     {"config_tracer_adv_order", 2, 0}, {"config_positive_definite", 0, 0},
     {"config_monotonic", 0, 0}, {"config_wind_stress", 0, 0}, {"config_bottom_drag", 0, 0},
     {"config_apvm_upwinding", 0.5, 0}, {"config_num_halos", 2, 0},
+    // tracer transport in sw_rk4 (no counterpart in the reference, which leaves it out): off
+    {"config_advect_tracers", 0, 0},
     // :45-55 dimensions
     {"nvertlevels", 1, 0}, {"ncells", 0, 0}, {"nedges", 0, 0}, {"nvertices", 0, 0},
     {"ntracers", 0, 0}, {"cellstart", 0, 0}, {"cellend", 0, 0}, {"vertexstart", 0, 0},
@@ -203,6 +205,7 @@ Engine::~Engine() {
     if (v.dev) cudaFree(v.dev);
   free_device_mesh();
   for (void *p : work) cudaFree(p);
+  if (trc) cudaFree(trc);
   window_free();
   for (cudaEvent_t ev : {ev_fork, ev_step, ev_join})
     if (ev) cudaEventDestroy(ev);
@@ -673,12 +676,83 @@ static void rk_coeffs(double dt, double w[4], double c[4]) {
   c[0] = dt / 2.; c[1] = dt / 2.; c[2] = dt; c[3] = 0.;
 }
 
+// ---- tracer transport -------------------------------------------------------------------
+bool Engine::tracers_advected() {
+  if (sc("config_advect_tracers") == 0.0 || nT <= 0) return false;
+  if (!var("tracers").allocated) throw EngineError(MPSW_ERR_STATE, "tracers are not allocated");
+  if (sc("config_tracer_adv_order") != 2.0 || sc("config_h_tracer_eddy_diff2") != 0.0 ||
+      sc("config_h_tracer_eddy_diff4") != 0.0)
+    throw EngineError(MPSW_ERR_UNSUPPORTED, "tracer transport supports config_tracer_adv_order 2 without eddy diffusion");
+  return true;
+}
+
+// six [nT][nC] device blocks, reallocated (and the step graphs dropped) when nT or nC changes
+double *Engine::tracer_bufs() {
+  const long long n = 6LL * nT * nC;
+  if (trc_n != n) {
+    graphs_free();
+    if (trc) cudaFree(trc);
+    trc = (double *)dalloc(sizeof(double) * n);
+    trc_n = n;
+  }
+  return trc;
+}
+
+// tracers(1, :, 1, c) -> [nT][nC] in internal cell order
+void Engine::tracers_upload(double *dst) {
+  const Var &v = var("tracers");
+  const auto &p = perm_of(1);
+  staging.assign((size_t)nT * nC, 0.0);
+  for (int i = 0; i < nC; i++)
+    for (int t = 0; t < nT; t++) staging[(size_t)t * nC + p[i]] = v.hr[2 * ((size_t)t + (size_t)nT * i)];
+  cuda_check(cudaMemcpyAsync(dst, staging.data(), sizeof(double) * staging.size(), cudaMemcpyHostToDevice, stream),
+             "tracers upload");
+  cuda_check(cudaStreamSynchronize(stream), "tracers upload");
+}
+
+// both time levels of tracers and tend_tracer (the last stage's tendency) back into the module
+void Engine::tracers_download(const double *src, const double *tend) {
+  const auto &p = perm_of(1);
+  Var &v = var("tracers");
+  staging.resize((size_t)nT * nC);
+  cuda_check(cudaMemcpyAsync(staging.data(), src, sizeof(double) * staging.size(), cudaMemcpyDeviceToHost, stream),
+             "tracers download");
+  cuda_check(cudaStreamSynchronize(stream), "tracers download");
+  for (int i = 0; i < nC; i++)
+    for (int t = 0; t < nT; t++) {
+      const double x = staging[(size_t)t * nC + p[i]];
+      v.hr[2 * ((size_t)t + (size_t)nT * i)] = x;
+      v.hr[2 * ((size_t)t + (size_t)nT * i) + 1] = x;
+    }
+  v.nonzero = true;
+  Var &tt = var("tend_tracer");
+  if (!tt.allocated) return;
+  cuda_check(cudaMemcpyAsync(staging.data(), tend, sizeof(double) * staging.size(), cudaMemcpyDeviceToHost, stream),
+             "tend_tracer download");
+  cuda_check(cudaStreamSynchronize(stream), "tend_tracer download");
+  for (int i = 0; i < nC; i++)
+    for (int t = 0; t < nT; t++) tt.hr[(size_t)t + (size_t)nT * i] = staging[(size_t)t * nC + p[i]];
+  tt.nonzero = true;
+}
+
 void Engine::rk4(int nsteps) {  // src/mpas_sw_module.f90:528-635
   prepare();
   const Phys<double> ph = phys();
   double w[4], c[4];
   rk_coeffs(ph.dt, w, c);
   double *u0 = dv("u"), *h0 = dv("h");
+  // tracer transport (config_advect_tracers): tracers(1) on the device for the whole call,
+  // [nT][nC] blocks: the state, three provisional stages, the accumulator, the last tendency
+  const bool adv = tracers_advected();
+  double *tr0 = nullptr, *trp[3] = {}, *tracc = nullptr, *trtend = nullptr;
+  if (adv) {
+    tr0 = tracer_bufs();
+    const size_t n = (size_t)nT * nC;
+    for (int k = 0; k < 3; k++) trp[k] = tr0 + (k + 1) * n;
+    tracc = tr0 + 4 * n;
+    trtend = tr0 + 5 * n;
+    tracers_upload(tr0);
+  }
   auto step = [&]() {
     for (int k = 0; k < 4; k++) {
       const double *ui = k == 0 ? u0 : sp_u[k - 1];
@@ -686,11 +760,22 @@ void Engine::rk4(int nsteps) {  // src/mpas_sw_module.f90:528-635
       RK<double, double> ru{u0, k == 0 ? u0 : acc_u, k == 3 ? u0 : acc_u, k < 3 ? sp_u[k] : nullptr, c[k], w[k], 0.0, ph.tc1};
       RK<double, double> rh{h0, k == 0 ? h0 : acc_h, k == 3 ? h0 : acc_h, k < 3 ? sp_h[k] : nullptr, c[k], w[k], 0.0, 0};
       fwd_stage(ui, hi, stage[0], ph, ru, rh, k == 3 ? dv("tend_u") : nullptr, k == 3 ? dv("tend_h") : nullptr);
+      // after the stage: its h_edge is in stage[0], the next provisional h in sp_h[k] and, in
+      // stage 4, the new h in h0
+      if (adv)
+        L64::tracer_stage(m64, d_cnb, nT, ui, stage[0].he, k == 0 ? tr0 : trp[k - 1], tr0, h0, k < 3 ? sp_h[k] : h0,
+                          k == 3 ? trtend : nullptr, tracc, k < 3 ? trp[k] : nullptr, c[k], w[k], k == 0, k == 3,
+                          stream);
     }
   };
   // one CUDA graph per step (its buffers are fixed), captured on the first step
-  const GraphKey key = graph_key(8, 0, 1, u0, h0);
+  GraphKey key = graph_key(8, 0, 1, u0, h0);
+  if (adv) {
+    key.p3 = tr0;
+    key.n2 = nT;
+  }
   for (int n = 0; n < nsteps; n++) run_graph(key, step);
+  if (adv) tracers_download(tr0, trtend);
   finish_levels({"u", "h"});
   L64::recon(m64, 1, ph.sphere, u0, dv("uReconstructX"), dv("uReconstructY"), dv("uReconstructZ"),
              dv("uReconstructZonal"), dv("uReconstructMeridional"), stream);
@@ -715,6 +800,8 @@ void Engine::forward(int prec, int nsteps) {
   }
   if (prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   if (nsteps < 0) throw EngineError(MPSW_ERR_ARG, "nsteps must be >= 0");
+  if (tracers_advected())
+    throw EngineError(MPSW_ERR_UNSUPPORTED, "tracer transport (config_advect_tracers) runs with FP64 stencils only");
   prepare();
   const Phys<double> ph64 = phys();
   Phys<float> ph{};

@@ -130,6 +130,8 @@ struct Engine {
   double *tu_[2] = {}, *th_[2] = {}, *xacc_u = nullptr, *xacc_h = nullptr;
   Diag<float> d32{};                          // FP32-stencil forward (precision 1)
   float *s32_u[4] = {}, *s32_h[4] = {};
+  double *trc = nullptr;  // tracer transport work ([6][nT][nC]), see tracer_bufs
+  long long trc_n = 0;
   int pending_diag = 0;  // 1: diagnostics of the level-1 state owed, 2: and their tangents
   Phys<double> phys_cache{};  // physics scalars, refreshed whenever a scalar is assigned
   void refresh_phys();
@@ -169,6 +171,10 @@ struct Engine {
   void mark_diag(int g, bool lazy);
   void mark_recon(int g);
   Phys<double> phys() const;
+  bool tracers_advected();
+  double *tracer_bufs();
+  void tracers_upload(double *dst);
+  void tracers_download(const double *src, const double *tend);
   void fwd_diag(const double *u, const double *h, const Diag<double> &d, const Phys<double> &ph);
   void fwd_stage(const double *u, const double *h, const Diag<double> &d, const Phys<double> &ph,
                  const RK<double, double> &rku, const RK<double, double> &rkh, double *tu, double *th);

@@ -218,6 +218,41 @@ __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *
   }
 }
 
+// Tracer transport in one RK4 stage, the call the reference leaves out of sw_rk4
+// (src/mpas_sw_module.f90:587): MPAS's order-2 scalar tendency in the form of the thickness
+// tendency (:468-482) -- the h_edge-weighted flux of the edge-mean tracer, gathered in the
+// reference's scatter order and divided by areaCell -- then MPAS's mass-weighted RK4 update.
+// One thread per (tracer, cell); tracers are [nT][nC].  The stage input tr_in is advected by the
+// stage's u and h_edge (he).  first: acc = tr0 h0 + w tend; otherwise acc += w tend.  tr_next
+// (stages 1-3): (h0 tr0 + c tend) / h_next.  last (stage 4): tr0 = acc / h_next, h_next being the
+// new h.  tend (optional) receives the stage's tendency.
+template <typename R, int NC>
+__global__ void k_tracer_stage(MeshDev<R> m, const int *__restrict__ c_nb, int nT, const R *__restrict__ u,
+                               const R *__restrict__ he, const R *__restrict__ tr_in, R *tr0, const R *h0,
+                               const R *h_next, R *tend, R *acc, R *tr_next, R c, R w, int first, int last) {
+  const int nC = m.nC;
+  MPSW_GRID_LOOP(t, (long long)nT * nC) {
+    const int cc = (int)(t % nC);
+    const R *tr = tr_in + (t - cc);
+    const int n = ld(m.c_n, cc);
+    const R tc = tr[cc];
+    R sum = R(0);
+    MPSW_PADDED(k, NC, n) {
+      const int e = ld(m.c_es, (size_t)k * nC + cc);
+      const R s = R(m.c_esg[(size_t)k * nC + cc]);
+      const R flux = (ld(u, e) * ld(m.e_dv, e)) * ld(he, e);
+      const R tre = R(0.5) * (tc + tr[ld(c_nb, (size_t)k * nC + cc)]);
+      sum = sum + (-s) * (flux * tre);
+    }
+    const R td = sum / ld(m.c_area, cc);
+    if (tend) tend[t] = td;
+    const R a = first ? tr0[t] * h0[cc] + w * td : acc[t] + w * td;
+    if (tr_next) tr_next[t] = (h0[cc] * tr0[t] + c * td) / h_next[cc];
+    if (last) tr0[t] = a / h_next[cc];
+    else acc[t] = a;
+  }
+}
+
 // Stand-alone thickness tendency from a given h_edge (src/mpas_sw_dyncore.f90:468-482).
 template <typename R>
 __global__ void k_tend_h(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ he, R *tend_h) {

@@ -172,6 +172,14 @@ void Launch<R, A>::fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R 
   MPSW_BDISPATCH(m, launch_k(k_fwd_edge_tend<R, A, NB::e2>, launch_cfg(m.nE), s, m, u, h, off, d, ph, rk, tend_u));
 }
 template <typename R, typename A>
+void Launch<R, A>::tracer_stage(const MeshDev<R> &m, const int *c_nb, int nT, const R *u, const R *he,
+                                const R *tr_in, R *tr0, const R *h0, const R *h_next, R *tend, R *acc, R *tr_next,
+                                R c, R w, int first, int last, cudaStream_t s) {
+  g_launches++;
+  MPSW_BDISPATCH(m, launch_k(k_tracer_stage<R, NB::c>, launch_cfg((long long)nT * m.nC), s, m, c_nb, nT, u, he, tr_in,
+                             tr0, h0, h_next, tend, acc, tr_next, c, w, first, last));
+}
+template <typename R, typename A>
 void Launch<R, A>::tend_h(const MeshDev<R> &m, const R *u, const R *he, R *out, cudaStream_t s) {
   g_launches++;
   launch_k(k_tend_h<R>, launch_cfg(m.nC), s, m, u, he, out);

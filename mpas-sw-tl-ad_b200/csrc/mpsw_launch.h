@@ -55,6 +55,9 @@ struct Launch {
   static void fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                             const Phys<R> &ph, const RK<R, A> &rk, R *tend_u, cudaStream_t s);
   static void tend_h(const MeshDev<R> &m, const R *u, const R *he, R *out, cudaStream_t s);
+  static void tracer_stage(const MeshDev<R> &m, const int *c_nb, int nT, const R *u, const R *he, const R *tr_in,
+                           R *tr0, const R *h0, const R *h_next, R *tend, R *acc, R *tr_next, R c, R w, int first,
+                           int last, cudaStream_t s);
   static void recon(const MeshDev<R> &m, int B, int sphere, const R *u, R *X, R *Y, R *Z, R *Zon,
                     R *Mer, cudaStream_t s);
   // tangent linear, B members

@@ -29,6 +29,10 @@ printing instead of STOPping the interpreter; misuse raises RuntimeError/ValueEr
 engine's message instead of crashing; only global (closed-sphere) meshes with nVertLevels = 1
 and thickness_adv_order 2 are accepted (orders 3/4 are accepted while ``deriv_two`` is zero,
 where they coincide with order 2, as in the reference whose deriv_two is never filled).
+
+Extension: with ``config_advect_tracers = 1`` (default 0, the reference's behaviour of only
+carrying the tracers) ``sw_rk4`` and ``sw_rk4_steps(n, 0)`` also transport ``tracers`` (MPAS's
+order-2 scalar tendency with its mass-weighted RK4) and set ``tend_tracer``.
 """
 from __future__ import annotations
 
@@ -196,12 +200,17 @@ class MpasSwModule:
                   'edgenormalvectors', 'celltangentplane', 'coeffs_reconstruct'):
             self._pull(k)
 
+    def _tracers_advected(self):
+        return bool(self.config_advect_tracers) and self.__dict__['_arr'].get('tracers') is not None
+
     def sw_rk4(self):
-        self._run('mpsw_sw_rk4', 1, reads=_STATE, eager=_STATE,
-                  lazy=_DIAG + ('tend_u', 'tend_h'))
-        tr = self.__dict__['_arr'].get('tracers')
-        if tr is not None:
-            tr[1] = tr[0]
+        adv = self._tracers_advected()
+        tr = ('tracers',) if adv else ()
+        self._run('mpsw_sw_rk4', 1, reads=_STATE + tr, eager=_STATE + tr,
+                  lazy=_DIAG + ('tend_u', 'tend_h') + (('tend_tracer',) if adv else ()))
+        arr = self.__dict__['_arr'].get('tracers')
+        if arr is not None and not adv:
+            arr[1] = arr[0]
         self.rk_step = 5
 
     def sw_rk4_steps(self, nsteps, precision=0):
@@ -209,11 +218,14 @@ class MpasSwModule:
         precision 0 is bit-identical to repeated sw_rk4; precision 1 runs the stencils in FP32
         and keeps the state and its RK4 accumulation in FP64 (tend_u / tend_h are then left
         as they were)."""
-        self._run('mpsw_forward', int(precision), int(nsteps), reads=_STATE, eager=_STATE,
-                  lazy=_DIAG + (('tend_u', 'tend_h') if int(precision) == 0 else ()))
-        tr = self.__dict__['_arr'].get('tracers')
-        if tr is not None and nsteps > 0:
-            tr[1] = tr[0]
+        adv = self._tracers_advected()
+        tr = ('tracers',) if adv else ()
+        self._run('mpsw_forward', int(precision), int(nsteps), reads=_STATE + tr, eager=_STATE + tr,
+                  lazy=_DIAG + (('tend_u', 'tend_h') + (('tend_tracer',) if adv else ())
+                                if int(precision) == 0 else ()))
+        arr = self.__dict__['_arr'].get('tracers')
+        if arr is not None and nsteps > 0 and not adv:
+            arr[1] = arr[0]
         if nsteps > 0:
             self.rk_step = 5
 

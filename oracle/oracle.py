@@ -108,6 +108,7 @@ _INT_ARRAYS = {'boundaryCell', 'boundaryEdge', 'advCells', 'cellsOnCell', 'cells
                'verticesOnEdge', 'nEdgesOnCell', 'nEdgesOnEdge'}
 
 _SCALAR_DEFAULTS = {  # src/mpas_sw_module.f90:23-55
+    'config_advect_tracers': 0,  # tracer transport switch (off: tracers carried, as the reference)
     'config_test_case': 5, 'config_dt': 150.0, 'config_stats_interval': 100,
     'config_h_ScaleWithMesh': False, 'config_h_mom_eddy_visc2': 0.0,
     'config_h_mom_eddy_visc4': 0.0, 'config_h_tracer_eddy_diff2': 0.0,
@@ -259,6 +260,9 @@ class OracleModule:
 
     def solve_diagnostics_tlm(self):
         self._call('orc_solve_diagnostics_tlm')
+
+    def compute_scalar_tend(self):
+        self._call('orc_compute_scalar_tend')
 
     def compute_tend_tlm(self):
         self._call('orc_compute_tend_tlm')

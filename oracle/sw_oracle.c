@@ -388,6 +388,31 @@ static void tend_fwd(orc_mod *m, const double *h, const double *u, const double 
 /* ---------------------------------------------------------------------------------------- */
 /* Geometry + RBF reconstruction setup: src/mpas_sw_operators.f90:2-279, 413-625              */
 /* ---------------------------------------------------------------------------------------- */
+/* Tracer transport, the call the reference leaves out of its RK4 loop
+   (src/mpas_sw_module.f90:587, "call sw_compute_scalar_tend() ! omitted"): MPAS's
+   sw_compute_scalar_tend at advection order 2 (MPAS-Model shallow-water core, not vendored in
+   the reference), restated in the form of this file's thickness tendency (:468-482): the
+   h_edge-weighted flux of the edge-mean tracer, scattered to both cells of each edge in edge
+   order, divided by areaCell afterwards.  tr and tend are (nTracers, nCells), tracer fastest. */
+static void scalar_tend_fwd(orc_mod *m, const double *u, const double *h_edge, const double *tr,
+                            double *tend) {
+  const int nCells = IS(nCells), nEdges = IS(nEdges), nT = IS(nTracers);
+  const int *cellsOnEdge = I(cellsOnEdge);
+  const double *dvEdge = R(dvEdge), *areaCell = R(areaCell);
+  for (int i = 1; i <= nT * nCells; i++) A1(tend, i) = 0.0;
+  for (int iEdge = 1; iEdge <= nEdges; iEdge++) {
+    const int cell1 = A2(cellsOnEdge, 2, 1, iEdge), cell2 = A2(cellsOnEdge, 2, 2, iEdge);
+    const double flux = A1(u, iEdge) * A1(dvEdge, iEdge) * A1(h_edge, iEdge);
+    for (int t = 1; t <= nT; t++) {
+      const double tr_edge = 0.5 * (A2(tr, nT, t, cell1) + A2(tr, nT, t, cell2));
+      A2(tend, nT, t, cell1) = A2(tend, nT, t, cell1) - flux * tr_edge;
+      A2(tend, nT, t, cell2) = A2(tend, nT, t, cell2) + flux * tr_edge;
+    }
+  }
+  for (int iCell = 1; iCell <= nCells; iCell++)
+    for (int t = 1; t <= nT; t++) A2(tend, nT, t, iCell) = A2(tend, nT, t, iCell) / A1(areaCell, iCell);
+}
+
 static void unit_vec(double *x) { /* :118-127 */
   const double mag = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
   x[0] = x[0] / mag; x[1] = x[1] / mag; x[2] = x[2] / mag;
@@ -1413,20 +1438,43 @@ int orc_sw_rk4(orc_mod *m) { /* :528-635 */
   memcpy(u2, u1, sizeof(double) * nE);
   memcpy(h2, h1, sizeof(double) * nC);
   for (int i = 0; i < nT * nC; i++) A2(R(tracers), 2, 2, i + 1) = A2(R(tracers), 2, 1, i + 1);
+  /* tracer transport (opt-in, MPAS's mass-weighted RK4 of the tracers): provisional tracers
+     (h(1) tr(1) + substep * tend) / hProvis, accumulation of h(1) tr(1) + sum of weight * tend,
+     divided by h(2) at the end */
+  const int adv = IS(config_advect_tracers) != 0 && nT > 0;
+  double *t1 = NULL, *tP = NULL, *t2 = NULL, *tt = R(tend_tracer);
+  if (adv) {
+    t1 = dalloc((size_t)nT * nC); tP = dalloc((size_t)nT * nC); t2 = dalloc((size_t)nT * nC);
+    for (int i = 0; i < nT * nC; i++) t1[i] = tP[i] = A2(R(tracers), 2, 1, i + 1);
+    for (int c = 0; c < nC; c++)
+      for (int t = 0; t < nT; t++) t2[t + nT * c] = t1[t + nT * c] * h1[c];
+  }
   rk_weights[0] = dt / 6.; rk_weights[1] = dt / 3.; rk_weights[2] = dt / 3.; rk_weights[3] = dt / 6.;
   rk_substep_weights[0] = dt / 2.; rk_substep_weights[1] = dt / 2.; rk_substep_weights[2] = dt;
   rk_substep_weights[3] = 0.;
   for (int rk = 1; rk <= 4; rk++) {
     IS(rk_step) = rk;
     TEND_FWD(hP, uP);
+    if (adv) scalar_tend_fwd(m, uP, R(h_edge), tP, tt);
     if (rk < 4) {
       for (int e = 0; e < nE; e++) uP[e] = u1[e] + rk_substep_weights[rk - 1] * tu[e];
       for (int c = 0; c < nC; c++) hP[c] = h1[c] + rk_substep_weights[rk - 1] * th[c];
+      if (adv)
+        for (int c = 0; c < nC; c++)
+          for (int t = 0; t < nT; t++)
+            tP[t + nT * c] = (h1[c] * t1[t + nT * c] + rk_substep_weights[rk - 1] * tt[t + nT * c]) / hP[c];
     }
     if (IS(config_test_case) == 1) memcpy(uP, u1, sizeof(double) * nE);
     DIAG_FWD(hP, uP);
     for (int e = 0; e < nE; e++) u2[e] = u2[e] + rk_weights[rk - 1] * tu[e];
     for (int c = 0; c < nC; c++) h2[c] = h2[c] + rk_weights[rk - 1] * th[c];
+    if (adv)
+      for (int i = 0; i < nT * nC; i++) t2[i] = t2[i] + rk_weights[rk - 1] * tt[i];
+  }
+  if (adv) {
+    for (int c = 0; c < nC; c++)
+      for (int t = 0; t < nT; t++) A2(R(tracers), 2, 2, t + nT * c + 1) = t2[t + nT * c] / h2[c];
+    free(t1); free(tP); free(t2);
   }
   if (IS(config_test_case) == 1) memcpy(u2, u1, sizeof(double) * nE);
   DIAG_FWD(h2, u2);
@@ -1750,6 +1798,17 @@ int orc_compute_tend_adj(orc_mod *m) {
   free(h1); free(u1); free(h1a); free(u1a);
   return 0;
 }
+int orc_compute_scalar_tend(orc_mod *m) {
+  if (check(m)) return 1;
+  const int nC = IS(nCells), nE = IS(nEdges), nT = IS(nTracers);
+  double *u1 = dalloc(nE), *t1 = dalloc((size_t)nT * nC + 1);
+  get_level(R(u), nE, 1, u1);
+  for (int i = 0; i < nT * nC; i++) t1[i] = A2(R(tracers), 2, 1, i + 1);
+  scalar_tend_fwd(m, u1, R(h_edge), t1, R(tend_tracer));
+  free(u1); free(t1);
+  return 0;
+}
+
 int orc_reconstruct_2d(orc_mod *m) {
   if (check(m)) return 1;
   const int nE = IS(nEdges);

@@ -57,7 +57,7 @@ extern "C" {
   X(nCells) X(nEdges) X(nVertices) X(nVertLevels) X(nTracers) X(maxEdges) X(maxEdges2) \
   X(vertexDegree) X(R3) X(config_test_case) X(config_h_ScaleWithMesh) \
   X(config_thickness_adv_order) X(config_monotonic) X(config_wind_stress) \
-  X(config_bottom_drag) X(on_a_sphere) X(is_periodic) X(rk_step)
+  X(config_bottom_drag) X(on_a_sphere) X(is_periodic) X(rk_step) X(config_advect_tracers)
 
 /* real scalars */
 #define ORC_RSCAL(X) \
@@ -107,6 +107,7 @@ int orc_compute_tend_tlm(orc_mod *m);
 int orc_solve_diagnostics_adj(orc_mod *m);/* consumes module diag _ad, accumulates h_ad(1),u_ad(1) */
 int orc_compute_tend_adj(orc_mod *m);     /* consumes tend_*_ad, accumulates into module _ad */
 int orc_reconstruct_2d(orc_mod *m);
+int orc_compute_scalar_tend(orc_mod *m); /* tend_tracer(tracers(1), u(1), module h_edge) */
 
 #ifdef __cplusplus
 }

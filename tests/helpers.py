@@ -25,10 +25,10 @@ def configure(m, dt=600.0, visc2=0.0, visc4=0.0, drag=False, wind=False, tc=5, a
     m.config_apvm_upwinding = apvm
 
 
-def setup(m, level, case='tc5', seed=0, tl=False, ad=False, **cfg):
+def setup(m, level, case='tc5', seed=0, tl=False, ad=False, ntracers=1, **cfg):
     """Load mesh + initial condition into module `m` (oracle or engine) and run init_block."""
     msh = mesh(level)
-    O.load_mesh(m, msh)
+    O.load_mesh(m, msh, ntracers)
     configure(m, tc=5 if case == 'tc5' else (2 if case == 'tc2' else (1 if case == 'tc1' else 7)), **cfg)
     if case == 'tc5':
         m.sw_test_case_5()

@@ -224,3 +224,60 @@ def test_forward_fp32_stencils_close_to_fp64(phys):
     eu, eh = rel(b.u[0, 0], a.u[0, 0]), rel(b.h[0, 0], a.h[0, 0])
     assert eu < 1e-5 and eh < 1e-5, (eu, eh)
     assert not np.array_equal(a.h[0, 0], b.h[0, 0])  # the FP32 path did run
+
+
+# ---- tracer transport (config_advect_tracers; the reference leaves it out) -----------------
+def tracer_pair(level=3, ntr=2, seed=3, **kw):
+    o = setup(O.OracleModule(), level, 'tc5', ntracers=ntr, **kw)
+    rng = np.random.default_rng(seed)
+    o.tracers[0] = 1.0 + 0.1 * rng.standard_normal(o.tracers[0].shape)
+    o.tracers[1] = o.tracers[0]
+    g = clone(o, MpasSwModule(), **kw)
+    for m in (o, g):
+        m.config_advect_tracers = 1
+    return o, g
+
+
+@pytest.mark.parametrize('phys', [dict(), dict(visc2=2.0e5, visc4=1.0e15)])
+def test_tracer_transport_bit_identical(phys):
+    """sw_rk4 with tracer transport: tracers and tend_tracer equal the oracle's bit for bit, and
+    u, h are those of a run without transport."""
+    o, g = tracer_pair(**phys)
+    plain = clone(o, MpasSwModule(), **phys)
+    plain.config_advect_tracers = 0
+    for _ in range(3):
+        o.sw_rk4()
+        g.sw_rk4()
+        plain.sw_rk4()
+    assert o.tracers.shape[1] == 2
+    assert np.array_equal(g.tracers, o.tracers)
+    assert np.array_equal(g.tend_tracer, o.tend_tracer)
+    assert not np.array_equal(g.tracers[0], plain.tracers[0])  # the tracers did move
+    assert np.array_equal(g.u, plain.u) and np.array_equal(g.h, plain.h)
+
+
+def test_tracer_transport_steps_and_conservation():
+    """sw_rk4_steps(n) with transport equals n sw_rk4 calls; on level 5 the tracer mass
+    sum(areaCell h tracer) is conserved to rounding and a constant tracer stays constant."""
+    o, g = tracer_pair(level=3)
+    g2 = clone(o, MpasSwModule())
+    g2.config_advect_tracers = 1
+    for _ in range(4):
+        g.sw_rk4()
+    g2.sw_rk4_steps(4)
+    assert np.array_equal(g.tracers, g2.tracers)
+    with pytest.raises(RuntimeError):
+        g2.sw_rk4_steps(1, precision=1)
+
+    m = setup(MpasSwModule(), 5, 'seeded', dt=300.0, ntracers=2)
+    m.tracers[0, 0, 0] = 1.0
+    x = np.asarray(m.xcell).ravel()
+    m.tracers[0, 1, 0] = 1.0 + 0.5 * x / np.abs(x).max()
+    m.config_advect_tracers = 1
+    area = np.asarray(m.areacell).ravel()
+    mass0 = (area * m.h[0, 0] * m.tracers[0, 1, 0]).sum()
+    m.sw_rk4_steps(20)
+    mass1 = (area * m.h[0, 0] * m.tracers[0, 1, 0]).sum()
+    assert abs(mass1 - mass0) / abs(mass0) < 1e-12
+    assert np.abs(m.tracers[0, 0, 0] - 1.0).max() < 1e-12
+    assert np.abs(m.tracers[0, 1, 0] - m.tracers[0, 1, 0].mean()).max() > 1e-3
