@@ -247,7 +247,9 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
                    + 2 * s * E                                                  # base u, h_edge
                    + B * (s * (E + C + V + 3 * C) + (a + 2 * s) * C),          # u,h,pv in; div,ke,pc out; RK
         'tl_edge_diag': eoe + (6 * i + 2 * s) * E + 4 * s * E                  # ends; dc,dv; base gradPVt,v,gradPVn,u
-                        + B * s * (E + C + V + C + 2 * E),                     # u,h,pv,pc in; pv_edge,h_edge out
+                        + (2 * s * E if s == 4 else 0)                         # FP32: base h_edge, pv_edge
+                        + B * s * (E + C + V + C + 2 * E)                      # u,h,pv,pc in; pv_edge,h_edge out
+                        + (B * s * E if s == 4 else 0),                        # FP32: h_edge -> u h_edge, + PV flux
         'tl_edge_tend': eoe + (2 * i + s) * E + 3 * s * E                      # c1,c2,dc; base pv_edge,u,h_edge
                         + B * (s * (3 * E + 2 * C) + (a + 2 * s) * E),         # u,pe,he,ke,h in; RK
         'ad_edge': eoe + s * S + (2 * i + s) * E + 6 * s * E                   # wrev; c1,c2,dv; 6 base fields

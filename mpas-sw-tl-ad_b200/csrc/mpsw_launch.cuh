@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <initializer_list>
+#include <stdexcept>
 #include <utility>
 
 #include "mpsw_kernels.cuh"
@@ -217,6 +218,7 @@ template <typename R, typename A>
 void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                                 const Diag<R> &d, const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
+  if (sizeof(R) == 4 && !d.v) throw std::invalid_argument("FP32 tl_edge_diag needs rows for the PV flux in d.v");
   Diag<R> dd = d;
   if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
   const int v = vec_width<R, A>(B, {ut, ht, dd.pvv, dd.pc, dd.div, dd.vort, dd.pe, dd.he, dd.v, dd.gpt, dd.gpn, dd.dsq_u},
@@ -235,7 +237,8 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
                                 const Diag<R> &d, const Phys<R> &ph, const RK<R, A> &rk, R *tend_u,
                                 cudaStream_t s) {
   g_launches++;
-  const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
+  if (sizeof(R) == 4 && !d.v) throw std::invalid_argument("FP32 tl_edge_tend needs the PV-flux rows in d.v");
+  const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.v, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
                                     rk.x0, rk.acc_in, rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1],
                                     rk.t_in[2]},
                                 tuned_v(K_TL_EDGE_TEND));

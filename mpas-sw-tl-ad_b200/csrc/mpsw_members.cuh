@@ -467,8 +467,17 @@ __device__ __forceinline__ void tl_edge_diag_body(const MeshDev<R> &m, int B, co
   pet = pet - ((ph.apvm * uet) * ph.dt) * ld(bs.gpn, e) - ((ph.apvm * ld(bs.u, e)) * ph.dt) * gpnt;
   const size_t o = (size_t)e * B + b;
   stv<V>(d.pe + o, pet);
-  stv<V>(d.he + o, R(0.5) * (ldv<V>(ht + (size_t)c1 * B + b) + ldv<V>(ht + (size_t)c2 * B + b)));
-  if (d.v) stv<V>(d.v + o, vt);
+  const M het = R(0.5) * (ldv<V>(ht + (size_t)c1 * B + b) + ldv<V>(ht + (size_t)c2 * B + b));
+  if constexpr (sizeof(R) == 4) {
+    // FP32 members: the edge's tangent thickness flux (u h_edge)' in d.he and tangent PV flux
+    // (u h_edge pv_edge)' in d.v, the two rows tl_edge_tend gathers at the neighbours
+    const R ub = ld(bs.u, e), hb = ld(bs.he, e), pb = ld(bs.pe, e);
+    stv<V>(d.he + o, uet * hb + ub * het);
+    stv<V>(d.v + o, (uet * hb) * pb + (ub * hb) * pet + (ub * pb) * het);
+  } else {
+    stv<V>(d.he + o, het);
+    if (d.v) stv<V>(d.v + o, vt);
+  }
   if (d.gpt) stv<V>(d.gpt + o, gptt);
   if (d.gpn) stv<V>(d.gpn + o, gpnt);
   if (d.dsq_u)
@@ -509,14 +518,30 @@ __device__ __forceinline__ void tl_edge_tend_body(const MeshDev<R> &m, int B, co
   const M pet_e = ldv<V>(d.pe + (size_t)e * B + b);
   const R pe_e = ld(bs.pe, e);
   M qt = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n) {
-    const int eoe = l.nb(j);
-    const R w = l.w(j);
-    const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + b));
-    const R wpv = R(0.5) * (pe_e + l.f(0, j));
-    const R ub = l.f(1, j), heb = l.f(2, j);
-    qt = qt + ((w * ldv<V>(ut + (size_t)eoe * B + b)) * wpv) * heb + ((w * ub) * wpvt) * heb +
-         ((w * ub) * wpv) * ldv<V>(d.he + (size_t)eoe * B + b);
+  if constexpr (sizeof(R) == 4) {
+    // FP32 members: q' = 0.5 pv_edge(e) sum w (u h_edge)'_j + 0.5 sum w (u h_edge pv_edge)'_j
+    //                  + 0.5 pv_edge'(e) sum w u_j h_edge_j, the same sum regrouped by the
+    // neighbour fluxes tl_edge_diag leaves in d.he and d.v: two member rows per neighbour
+    M f1 = mv_fill<R, V>(R(0)), f2 = mv_fill<R, V>(R(0));
+    R sb = R(0);
+    MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n) {
+      const size_t on = (size_t)l.nb(j) * B + b;
+      const R w = l.w(j);
+      f1 = f1 + w * ldv<V>(d.he + on);
+      f2 = f2 + w * ldv<V>(d.v + on);
+      sb = sb + (w * l.f(1, j)) * l.f(2, j);
+    }
+    qt = (R(0.5) * pe_e) * f1 + R(0.5) * f2 + (R(0.5) * sb) * pet_e;
+  } else {
+    MPSW_SLOTS(j, NMAX, L::kPadded ? NMAX : n) {
+      const int eoe = l.nb(j);
+      const R w = l.w(j);
+      const M wpvt = R(0.5) * (pet_e + ldv<V>(d.pe + (size_t)eoe * B + b));
+      const R wpv = R(0.5) * (pe_e + l.f(0, j));
+      const R ub = l.f(1, j), heb = l.f(2, j);
+      qt = qt + ((w * ldv<V>(ut + (size_t)eoe * B + b)) * wpv) * heb + ((w * ub) * wpvt) * heb +
+           ((w * ub) * wpv) * ldv<V>(d.he + (size_t)eoe * B + b);
+    }
   }
   const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
   const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
@@ -535,7 +560,8 @@ __device__ __forceinline__ void tl_edge_tend_body(const MeshDev<R> &m, int B, co
     tut = tut - ud;
   }
   const R hh = ld(bs.he, e);
-  const M het = ldv<V>(d.he + (size_t)e * B + b);
+  // h_edge' of the edge itself (d.he holds the thickness flux for FP32 members)
+  const M het = R(0.5) * (ldv<V>(ht + (size_t)c1 * B + b) + ldv<V>(ht + (size_t)c2 * B + b));
   if (ph.wind) tut = tut - ((het * ld(m.e_usrc, e)) / R(RHO_REF)) / (hh * hh);
   if (ph.drag) {
     const M ket_e = R(0.5) * (ldv<V>(d.ke + (size_t)c1 * B + b) + ldv<V>(d.ke + (size_t)c2 * B + b));

@@ -70,8 +70,10 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   d.circ = nullptr;
   d.vort = walloc<R>(M, V, s); d.hv = nullptr; d.pvv = walloc<R>(M, V, s);
   d.div = walloc<R>(M, C, s); d.ke = walloc<R>(M, C, s); d.pc = walloc<R>(M, C, s); d.vc = nullptr;
-  d.v = nullptr; d.gpt = nullptr; d.gpn = nullptr;
+  d.gpt = nullptr; d.gpn = nullptr;
   d.pe = walloc<R>(M, Ed, s); d.he = walloc<R>(M, Ed, s);
+  // FP32 members keep the tangent PV flux in d.v (read by tl_edge_tend); FP64 needs no v'
+  d.v = sizeof(R) == 4 ? walloc<R>(M, Ed, s) : nullptr;
   d.dsq_u = walloc<R>(M, Ed, s); d.dsq_vort = walloc<R>(M, V, s); d.dsq_div = walloc<R>(M, C, s);
   for (int k = 0; k < 3; k++) {
     mb->pu[k] = walloc<R>(M, Ed, s);
