@@ -165,8 +165,17 @@ __global__ void k_fwd_edge_diag(MeshDev<R> m, const R *__restrict__ u, const R *
     const R gpn = (d.pc[c2] - d.pc[c1]) / dc;
     pe = pe - ((ph.apvm * ld(u, e)) * ph.dt) * gpn;
     d.pe[e] = pe;
-    d.he[e] = R(0.5) * ((ld(h, c1) + off) + (ld(h, c2) + off));
-    if (d.v) d.v[e] = v;
+    const R he = R(0.5) * ((ld(h, c1) + off) + (ld(h, c2) + off));
+    if constexpr (sizeof(R) == 4) {
+      // FP32 stencils: the edge's thickness flux u h_edge in d.he and PV flux u h_edge pv_edge
+      // in d.v, the two values k_fwd_edge_tend gathers at the neighbours
+      const R f = ld(u, e) * he;
+      d.he[e] = f;
+      d.v[e] = f * pe;
+    } else {
+      d.he[e] = he;
+      if (d.v) d.v[e] = v;
+    }
     if (d.gpt) d.gpt[e] = gpt;
     if (d.gpn) d.gpn[e] = gpn;
     if (d.dsq_u) d.dsq_u[e] = (d.div[c2] - d.div[c1]) / dc - (d.vort[v2] - d.vort[v1]) / dv;
@@ -183,10 +192,23 @@ __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *
     const int n = ld(m.e_n, e);
     const R pee = d.pe[e];
     R q = R(0);
-    MPSW_PADDED(j, NE, n) {
-      const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
-      const R wpv = R(0.5) * (pee + d.pe[eoe]);
-      q = q + ((ld(m.e_w, (size_t)j * nE + e) * ld(u, eoe)) * wpv) * d.he[eoe];
+    if constexpr (sizeof(R) == 4) {
+      // FP32 stencils: q = 0.5 pv_edge(e) sum w (u h_edge)_j + 0.5 sum w (u h_edge pv_edge)_j,
+      // the same sum regrouped by the neighbour fluxes k_fwd_edge_diag leaves in d.he and d.v
+      R f1 = R(0), f2 = R(0);
+      MPSW_PADDED(j, NE, n) {
+        const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
+        const R w = ld(m.e_w, (size_t)j * nE + e);
+        f1 = f1 + w * d.he[eoe];
+        f2 = f2 + w * d.v[eoe];
+      }
+      q = (R(0.5) * pee) * f1 + R(0.5) * f2;
+    } else {
+      MPSW_PADDED(j, NE, n) {
+        const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
+        const R wpv = R(0.5) * (pee + d.pe[eoe]);
+        q = q + ((ld(m.e_w, (size_t)j * nE + e) * ld(u, eoe)) * wpv) * d.he[eoe];
+      }
     }
     const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
     const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
@@ -207,10 +229,12 @@ __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *
       ud = (ld(m.e_sc4, e) * ph.visc4) * ud;
       tu = tu - ud;
     }
-    if (ph.wind) tu = tu + (ld(m.e_usrc, e) / R(RHO_REF)) / d.he[e];
+    // h_edge of the edge itself (d.he holds the thickness flux with FP32 stencils)
+    const R hee = sizeof(R) == 4 ? R(0.5) * ((ld(h, c1) + off) + (ld(h, c2) + off)) : d.he[e];
+    if (ph.wind) tu = tu + (ld(m.e_usrc, e) / R(RHO_REF)) / hee;
     if (ph.drag) {
       const R kee = R(0.5) * (d.ke[c1] + d.ke[c2]);
-      tu = tu - ((R(1.0e-3) * ld(u, e)) * sqrt(R(2) * kee)) / d.he[e];
+      tu = tu - ((R(1.0e-3) * ld(u, e)) * sqrt(R(2) * kee)) / hee;
     }
     if (tend_u) tend_u[e] = tu;
     if (rk.next) rk.next[e] = rk.frozen ? R(rk.x0[e]) : R(rk.x0[e] + rk.c * A(tu));

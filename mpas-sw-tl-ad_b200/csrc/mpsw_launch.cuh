@@ -155,6 +155,7 @@ template <typename R, typename A>
 void Launch<R, A>::fwd_edge_diag(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                                  const Phys<R> &ph, cudaStream_t s) {
   g_launches++;
+  if (sizeof(R) == 4 && !d.v) throw std::invalid_argument("FP32 fwd_edge_diag needs rows for the PV flux in d.v");
   Diag<R> dd = d;
   if (!(ph.visc4 > R(0))) dd.dsq_u = nullptr;  // delsq_u only feeds the del4 term
   MPSW_BDISPATCH(m, launch_k(k_fwd_edge_diag<R, NB::e2>, launch_cfg(m.nE), s, m, u, h, off, dd, ph));
@@ -170,6 +171,7 @@ template <typename R, typename A>
 void Launch<R, A>::fwd_edge_tend(const MeshDev<R> &m, const R *u, const R *h, R off, const Diag<R> &d,
                                  const Phys<R> &ph, const RK<R, A> &rk, R *tend_u, cudaStream_t s) {
   g_launches++;
+  if (sizeof(R) == 4 && !d.v) throw std::invalid_argument("FP32 fwd_edge_tend needs the PV-flux rows in d.v");
   MPSW_BDISPATCH(m, launch_k(k_fwd_edge_tend<R, A, NB::e2>, launch_cfg(m.nE), s, m, u, h, off, d, ph, rk, tend_u));
 }
 template <typename R, typename A>
