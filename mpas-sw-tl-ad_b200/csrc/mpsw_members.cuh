@@ -392,7 +392,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
       dve = ld(m.e_dv, e);
       heb = ld(bs.he, e);
       ub = ld(bs.u, e);
-      eo = ld(m.c_eoc, (size_t)k * nC + c);
+      // FP32 members take ke's terms in the scatter order, from the same edge loads
+      eo = sizeof(R) == 4 ? e : ld(m.c_eoc, (size_t)k * nC + c);
       k1 = (R(0.25) * ld(m.e_dc, eo)) * ld(m.e_dv, eo);
       k2 = R(2) * ld(bs.u, eo);
       v = ld(m.c_vs, (size_t)k * nC + c);
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
   if (lc >= cpb || c >= nC) return;
   const int b = (threadIdx.x - lc * tpe) * V;
   const M htc = ldv<V>(ht + (size_t)c * B + b);
-  M div = mv_fill<R, V>(R(0)), th = mv_fill<R, V>(R(0));
+  M div = mv_fill<R, V>(R(0)), th = mv_fill<R, V>(R(0)), ke = mv_fill<R, V>(R(0));
   MPSW_SLOTS(k, S, S) {
     const int i = k * cpb + lc;
     const R s = sr[0 * SC + i], dve = sr[1 * SC + i];
@@ -417,13 +418,15 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
     const M het = R(0.5) * (htc + ldv<V>(ht + (size_t)si[1 * SC + i] * B + b));
     const M flux = (ue * dve) * sr[2 * SC + i] + (sr[3 * SC + i] * dve) * het;
     th = th + (-s) * flux;
+    if constexpr (sizeof(R) == 4) ke = ke + sr[4 * SC + i] * (sr[5 * SC + i] * ue);
   }
   const R area = ld(m.c_area, c);
   div = div * (R(1) / area);
-  M ke = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(k, S, S) {
-    const int i = k * cpb + lc;
-    ke = ke + sr[4 * SC + i] * (sr[5 * SC + i] * ldv<V>(ut + (size_t)si[2 * SC + i] * B + b));
+  if constexpr (sizeof(R) != 4) {
+    MPSW_SLOTS(k, S, S) {
+      const int i = k * cpb + lc;
+      ke = ke + sr[4 * SC + i] * (sr[5 * SC + i] * ldv<V>(ut + (size_t)si[2 * SC + i] * B + b));
+    }
   }
   ke = ke / area;
   M pc = mv_fill<R, V>(R(0)), vc = mv_fill<R, V>(R(0));
