@@ -157,10 +157,13 @@ __global__ void k_fwd_edge_diag(MeshDev<R> m, const R *__restrict__ u, const R *
       v = v + ld(m.e_w, (size_t)j * nE + e) * ld(u, ld(m.e_eoe, (size_t)j * nE + e));
     const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
     const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
-    const R gpt = (d.pvv[v2] - d.pvv[v1]) / dv;
+    const R pv1 = d.pvv[v1], pv2 = d.pvv[v2];
+    const R gpt = (pv2 - pv1) / dv;
+    // pv_edge's two vertex terms: the reference adds them over edgesOnVertex, which lists the
+    // same two endpoints; a sum of two terms is the same in either order
     R pe = R(0);
-    pe = pe + R(0.5) * d.pvv[ld(m.e_va, e)];
-    pe = pe + R(0.5) * d.pvv[ld(m.e_vb, e)];
+    pe = pe + R(0.5) * pv1;
+    pe = pe + R(0.5) * pv2;
     pe = pe - ((ph.apvm * v) * ph.dt) * gpt;
     const R gpn = (d.pc[c2] - d.pc[c1]) / dc;
     pe = pe - ((ph.apvm * ld(u, e)) * ph.dt) * gpn;

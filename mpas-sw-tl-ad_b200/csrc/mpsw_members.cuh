@@ -460,10 +460,13 @@ __device__ __forceinline__ void tl_edge_diag_body(const MeshDev<R> &m, int B, co
     vt = vt + l.w(j) * ldv<V>(ut + (size_t)l.nb(j) * B + b);
   const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
   const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
-  const M gptt = (ldv<V>(d.pvv + (size_t)v2 * B + b) - ldv<V>(d.pvv + (size_t)v1 * B + b)) / dv;
+  const M pv1 = ldv<V>(d.pvv + (size_t)v1 * B + b), pv2 = ldv<V>(d.pvv + (size_t)v2 * B + b);
+  const M gptt = (pv2 - pv1) / dv;
+  // pv_edge's two vertex terms: the reference adds them over edgesOnVertex, which lists the same
+  // two endpoints; a sum of two terms is the same in either order, so the loaded rows serve
   M pet = mv_fill<R, V>(R(0));
-  pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_va, e) * B + b);
-  pet = pet + R(0.5) * ldv<V>(d.pvv + (size_t)ld(m.e_vb, e) * B + b);
+  pet = pet + R(0.5) * pv1;
+  pet = pet + R(0.5) * pv2;
   pet = pet - ((ph.apvm * vt) * ph.dt) * ld(bs.gpt, e) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * gptt;
   const M gpnt = (ldv<V>(d.pc + (size_t)c2 * B + b) - ldv<V>(d.pc + (size_t)c1 * B + b)) / dc;
   const M uet = ldv<V>(ut + (size_t)e * B + b);
