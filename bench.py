@@ -268,19 +268,25 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
 
 def traffic_of(kernel, level, B):
     """DRAM bytes (read + write) of one launch of `kernel`, from the committed ncu summary of
-    that kernel on this workload (profiles/k_<kernel>_l<level>_b<B>_fp32.md), or None."""
+    that kernel on this workload (profiles/k_<kernel>_l<level>_b<B>_fp32.md: the read and write
+    sums, or the bytes derived from the DRAM rate and the duration), or None."""
     import re
     path = os.path.join(ROOT, 'profiles', 'k_%s_l%d_b%d_fp32.md' % (kernel, level, B))
     if not os.path.exists(path):
         return None
     unit = {'byte': 1, 'Kbyte': 1e3, 'Mbyte': 1e6, 'Gbyte': 1e9}
     total, found = 0.0, 0
+    derived = None
     for line in open(path):
         m = re.search(r'dram__bytes_(read|write)\.sum`?\)?\s*\|\s*([0-9.]+)\s*(\w+)', line)
         if m and m.group(3) in unit:
             total += float(m.group(2)) * unit[m.group(3)]
             found += 1
-    return total if found == 2 else None
+        # captures with sections only: bytes = dram__bytes.sum.per_second x duration
+        m = re.search(r'derived \(`dram__bytes\.sum\.per_second` . `gpu__time_duration\.sum`\)\s*\|\s*([0-9.]+)\s*(\w+)', line)
+        if m and m.group(2) in unit:
+            derived = float(m.group(1)) * unit[m.group(2)]
+    return total if found == 2 else derived
 
 
 def run_mpsw(a, rank, world):
