@@ -64,7 +64,12 @@ int mpsw_var_allocation(mpsw_handle *h);      /* :211-367 */
 int mpsw_var_allocation_tlm(mpsw_handle *h);  /* :369-429 */
 int mpsw_var_allocation_adj(mpsw_handle *h);  /* :431-493 */
 int mpsw_sw_mpas_init_block(mpsw_handle *h);  /* :495-526 */
-int mpsw_sw_rk4(mpsw_handle *h, int nsteps);      /* :528-635, nsteps consecutive calls */
+/* :528-635, nsteps consecutive calls.  Tracers are carried unchanged, as in the reference,
+ * unless the module scalar config_advect_tracers is nonzero (no counterpart in the reference):
+ * then tracers(1) are transported with the flow (MPAS's order-2 scalar tendency, the call the
+ * reference leaves out at :587, and its mass-weighted RK4), both levels of tracers receive the
+ * result and tend_tracer the last stage's tendency.  mpsw_forward precision 1 refuses it. */
+int mpsw_sw_rk4(mpsw_handle *h, int nsteps);
 int mpsw_sw_rk4_tlm(mpsw_handle *h, int nsteps);  /* :637-781 */
 int mpsw_sw_rk4_adj(mpsw_handle *h);              /* :783-1002 */
 /* nsteps RK4 steps of the level-1 state, as nsteps calls of sw_rk4 (:528-635).  precision 0:
