@@ -199,6 +199,11 @@ void Launch<R, A>::tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, cons
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.circ, d.vort, d.hv, d.pvv}, tuned_v(K_TL_VERTEX));
   const int bk = tuned_block(K_TL_VERTEX);
+  if (use_staged(m, B, v, vertex_stage_bytes<R>(), bk)) {
+    MPSW_VDISPATCH(v, launch_k(k_tl_vertex_st<R, VV>, staged_cfg(m.nV, B, VV, vertex_stage_bytes<R>(), bk), s, m, B,
+                               bs, ut, ht, d));
+    return;
+  }
   MPSW_VDISPATCH(v, (launch_k(k_tl_vertex<R, VV>, launch_cfg((long long)(m.nV) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, d)));
 }
 template <typename R, typename A>

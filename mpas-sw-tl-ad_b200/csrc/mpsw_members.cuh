@@ -303,6 +303,67 @@ __global__ void k_tl_vertex(MeshDev<R> m, int B, Base<R> bs, const R *__restrict
   }
 }
 
+// Shared-memory bytes per vertex of k_tl_vertex_st's stage: 3 slots of 2 indices and 3 values.
+template <typename R>
+__host__ __device__ constexpr size_t vertex_stage_bytes() {
+  return (size_t)VDEG * (2 * sizeof(int) + 3 * sizeof(R));
+}
+
+// k_tl_vertex with each block's vertex lists (edge, sign and dcEdge in the reference's scatter
+// order; cell and kite) copied into shared memory before waiting for the previous kernel: they
+// are mesh data, which no kernel writes.  Same operations as k_tl_vertex.
+template <typename R, int V>
+__global__ void k_tl_vertex_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                               const R *__restrict__ ht, Diag<R> d) {
+  using M = Mv<R, V>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nV = m.nV, tpe = B / V, vpb = blockDim.x / tpe;
+  const int v0 = blockIdx.x * vpb;
+  const size_t SV = (size_t)VDEG * vpb;
+  R *ssg = reinterpret_cast<R *>(smem_raw), *sdc = ssg + SV, *skt = sdc + SV;  // [VDEG][vpb] each
+  int *se = reinterpret_cast<int *>(skt + SV), *sc = se + SV;
+  for (int i = threadIdx.x; i < VDEG * vpb; i += blockDim.x) {
+    const int k = i / vpb, v = v0 + (i - k * vpb);
+    int e = 0, c = 0;
+    R sg = R(0), dc = R(0), kt = R(0);
+    if (v < nV) {
+      e = ld(m.v_es, (size_t)k * nV + v);
+      sg = R(m.v_esg[(size_t)k * nV + v]);
+      dc = ld(m.e_dc, e);
+      c = ld(m.v_c, (size_t)k * nV + v);
+      kt = ld(m.v_k, (size_t)k * nV + v);
+    }
+    ssg[i] = sg; sdc[i] = dc; skt[i] = kt; se[i] = e; sc[i] = c;
+  }
+  __syncthreads();
+  pdl_begin();
+  const int lv = threadIdx.x / tpe, v = v0 + lv;
+  if (lv >= vpb || v >= nV) return;
+  const int b = (threadIdx.x - lv * tpe) * V;
+  M circ = mv_fill<R, V>(R(0));
+#pragma unroll
+  for (int k = 0; k < VDEG; k++) {
+    const int i = k * vpb + lv;
+    circ = circ + ssg[i] * (sdc[i] * ldv<V>(ut + (size_t)se[i] * B + b));
+  }
+  const R area = ld(m.v_area, v);
+  const M vort = circ / area;
+  M hvt = mv_fill<R, V>(R(0));
+#pragma unroll
+  for (int k = 0; k < VDEG; k++) {
+    const int i = k * vpb + lv;
+    hvt = hvt + ldv<V>(ht + (size_t)sc[i] * B + b) * skt[i];
+  }
+  hvt = hvt / area;
+  const R hv = ld(bs.hv, v);
+  const M pvt = vort / hv - (hvt * (ld(m.v_f, v) + ld(bs.vort, v))) / (hv * hv);
+  const size_t o = (size_t)v * B + b;
+  if (d.circ) stv<V>(d.circ + o, circ);
+  stv<V>(d.vort + o, vort);
+  if (d.hv) stv<V>(d.hv + o, hvt);
+  stv<V>(d.pvv + o, pvt);
+}
+
 // :274-316, :397-421, thickness tendency :541-561 and the RK update.  In FP32 the kernel is held
 // to 48 registers (5 blocks of 256 threads per SM), which measured faster than the 56 it takes
 // otherwise.
