@@ -304,7 +304,15 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
         launch_k(k_ad_cell<R, A, V, NB>, launch_cfg((long long)(m.nC) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
       break;
     }
-    case 2: launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V)), tuned_block(K_AD_VERTEX)), s, m, B, bs, ph, in, sd, w); break;
+    case 2: {
+      const int bk = tuned_block(K_AD_VERTEX);
+      if (use_staged(m, B, V, ad_vertex_stage_bytes<R>(), bk))
+        launch_k(k_ad_vertex_st<R, A, V>, staged_cfg(m.nV, B, V, ad_vertex_stage_bytes<R>(), bk), s, m, B, bs, ph, in,
+                 sd, w);
+      else
+        launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
+      break;
+    }
     case 3: {
       constexpr int J = BoundsNarrow::e2;
       constexpr size_t eb = eoe_stage_bytes<R, J, 2, 1>();

@@ -1033,6 +1033,84 @@ __global__ void k_ad_vertex(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R>
   }
 }
 
+// Shared-memory bytes per vertex of k_ad_vertex_st's stage: 3 slots of 3 indices and 4 values.
+template <typename R>
+__host__ __device__ constexpr size_t ad_vertex_stage_bytes() {
+  return (size_t)VDEG * (3 * sizeof(int) + 4 * sizeof(R));
+}
+
+// k_ad_vertex with each block's vertex lists (cell with kite / areaCell; edgesOnVertex edge;
+// edge in the reference's scatter order with its sign, dvEdge and del2 coefficient) copied into
+// shared memory before waiting for the previous kernel: they are mesh data, which no kernel
+// writes.  Same operations as k_ad_vertex.
+template <typename R, typename A, int V>
+__global__ void k_ad_vertex_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+                               AdWork<R> w) {
+  using M = Mv<R, V>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nV = m.nV, tpe = B / V, vpb = blockDim.x / tpe;
+  const int v0 = blockIdx.x * vpb;
+  const size_t SV = (size_t)VDEG * vpb;
+  R *ska = reinterpret_cast<R *>(smem_raw), *ssg = ska + SV, *sdv = ssg + SV, *sk2 = sdv + SV;  // [VDEG][vpb]
+  int *sc = reinterpret_cast<int *>(sk2 + SV), *sve = sc + SV, *ses = sve + SV;
+  for (int i = threadIdx.x; i < VDEG * vpb; i += blockDim.x) {
+    const int k = i / vpb, v = v0 + (i - k * vpb);
+    int c = 0, ve = 0, e = 0;
+    R ka = R(0), sg = R(0), dve = R(1), k2 = R(0);
+    if (v < nV) {
+      c = ld(m.v_c, (size_t)k * nV + v);
+      ka = ld(m.v_k, (size_t)k * nV + v) / ld(m.c_area, c);
+      ve = ld(m.v_e, (size_t)k * nV + v);
+      e = ld(m.v_es, (size_t)k * nV + v);
+      sg = R(m.v_esg[(size_t)k * nV + v]);
+      dve = ld(m.e_dv, e);
+      if (ph.visc2 > R(0)) k2 = ld(m.e_sc2, e) * ph.visc2;
+    }
+    ska[i] = ka; ssg[i] = sg; sdv[i] = dve; sk2[i] = k2; sc[i] = c; sve[i] = ve; ses[i] = e;
+  }
+  __syncthreads();
+  pdl_begin();
+  const int lv = threadIdx.x / tpe, v = v0 + lv;
+  if (lv >= vpb || v >= nV) return;
+  const int b = (threadIdx.x - lv * tpe) * V;
+  M pvv_ad = mv_fill<R, V>(sd.pvv ? sd.pvv[v] : R(0));
+  M vort_ad = mv_fill<R, V>(sd.vort ? sd.vort[v] : R(0));
+#pragma unroll
+  for (int k = 0; k < VDEG; k++) {
+    const int i = k * vpb + lv;
+    const R ka = ska[i];
+    if (sd.vc) vort_ad = vort_ad + ka * sd.vc[sc[i]];
+    pvv_ad = pvv_ad + ka * ldv<V>(w.pc_ad + (size_t)sc[i] * B + b);
+  }
+#pragma unroll
+  for (int k = 0; k < VDEG; k++)
+    pvv_ad = pvv_ad + R(0.5) * ldv<V>(w.pe_ad + (size_t)sve[k * vpb + lv] * B + b);
+#pragma unroll
+  for (int k = 0; k < VDEG; k++) {
+    const int i = k * vpb + lv;
+    const int e = ses[i];
+    const R sg = ssg[i], dve = sdv[i];
+    const size_t oe = (size_t)e * B + b;
+    const M gpt_ad = w.gpt_ad ? ldv<V>(w.gpt_ad + oe)
+                              : mv_fill<R, V>(R(0)) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * ldv<V>(w.pe_ad + oe);
+    pvv_ad = pvv_ad + sg * (gpt_ad / dve);
+    if (ph.visc2 > R(0)) {
+      const M ud2 = sk2[i] * ldv<V>(in.tu + oe);
+      vort_ad = vort_ad + (-sg) * (ud2 / dve);
+    }
+    if (ph.visc4 > R(0)) vort_ad = vort_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dve);
+  }
+  const R hv = ld(bs.hv, v), area = ld(m.v_area, v);
+  M hv_ad = mv_fill<R, V>(sd.hv ? sd.hv[v] : R(0));
+  hv_ad = hv_ad - ((ld(m.v_f, v) + ld(bs.vort, v)) / (hv * hv)) * pvv_ad;
+  vort_ad = vort_ad + pvv_ad / hv;
+  hv_ad = hv_ad / area;
+  const M circ_ad = mv_fill<R, V>(sd.circ ? sd.circ[v] : R(0)) + vort_ad / area;
+  const size_t o = (size_t)v * B + b;
+  stv<V>(w.hv_ad + o, hv_ad);
+  stv<V>(w.circ_ad + o, circ_ad);
+}
+
 template <typename R, typename A, int V>
 __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, size_t o, const Mv<R, V> &pad,
                                         R area) {
