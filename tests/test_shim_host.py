@@ -31,6 +31,9 @@ def test_attribute_protocol():
     assert float(m.config_dt) == 900.
     m.config_bottom_drag = True
     assert int(m.config_bottom_drag) == 1
+    assert int(m.config_advect_tracers) == 0   # tracers carried, as in the reference
+    m.config_advect_tracers = 1
+    assert int(m.config_advect_tracers) == 1 and m.tracers.shape == (2, 1, 1, 162)
     with pytest.raises(ValueError):
         m.cellsonedge = np.zeros((3, 480), dtype=np.int32)
     with pytest.raises(AttributeError):
