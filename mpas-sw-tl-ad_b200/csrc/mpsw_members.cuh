@@ -967,12 +967,23 @@ __global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R
     const R half = R(0.5) * (sg * sg);  // 0.5 (sg is +-1), or 0 in a padded slot
     const M Te = ldv<V>(in.tu + oe);
     const M gpn_ad = w.gpn_ad ? ldv<V>(w.gpn_ad + oe) : mv_fill<R, V>(R(0)) - sr[2 * SC + i] * ldv<V>(w.pe_ad + oe);
-    pc_ad = pc_ad + (-sg) * (gpn_ad / dce);
-    ke_ad = ke_ad + sg * (Te / dce);
-    hd = hd + sg * (sr[3 * SC + i] * Te);
-    if (ph.drag) ke_ad = ke_ad + R(0.5) * (sr[4 * SC + i] * Te);
-    if (ph.visc2 > R(0)) div_ad = div_ad + (-sg) * ((sr[5 * SC + i] * Te) / dce);
-    if (ph.visc4 > R(0)) div_ad = div_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dce);
+    if constexpr (sizeof(R) == 4) {
+      // FP32 members: the slot's sign over dcEdge formed once, no division per member
+      const R rs = sg / dce;
+      pc_ad = pc_ad - rs * gpn_ad;
+      ke_ad = ke_ad + rs * Te;
+      hd = hd + sg * (sr[3 * SC + i] * Te);
+      if (ph.drag) ke_ad = ke_ad + R(0.5) * (sr[4 * SC + i] * Te);
+      if (ph.visc2 > R(0)) div_ad = div_ad - (rs * sr[5 * SC + i]) * Te;
+      if (ph.visc4 > R(0)) div_ad = div_ad - rs * ldv<V>(w.du_ad + oe);
+    } else {
+      pc_ad = pc_ad + (-sg) * (gpn_ad / dce);
+      ke_ad = ke_ad + sg * (Te / dce);
+      hd = hd + sg * (sr[3 * SC + i] * Te);
+      if (ph.drag) ke_ad = ke_ad + R(0.5) * (sr[4 * SC + i] * Te);
+      if (ph.visc2 > R(0)) div_ad = div_ad + (-sg) * ((sr[5 * SC + i] * Te) / dce);
+      if (ph.visc4 > R(0)) div_ad = div_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dce);
+    }
     hd = hd + half * ldv<V>(w.he_ad + oe);
   }
   const R area = ld(m.c_area, c);
@@ -1093,12 +1104,20 @@ __global__ void k_ad_vertex_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn
     const size_t oe = (size_t)e * B + b;
     const M gpt_ad = w.gpt_ad ? ldv<V>(w.gpt_ad + oe)
                               : mv_fill<R, V>(R(0)) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * ldv<V>(w.pe_ad + oe);
-    pvv_ad = pvv_ad + sg * (gpt_ad / dve);
-    if (ph.visc2 > R(0)) {
-      const M ud2 = sk2[i] * ldv<V>(in.tu + oe);
-      vort_ad = vort_ad + (-sg) * (ud2 / dve);
+    if constexpr (sizeof(R) == 4) {
+      // FP32 members: the slot's sign over dvEdge formed once, no division per member
+      const R rs = sg / dve;
+      pvv_ad = pvv_ad + rs * gpt_ad;
+      if (ph.visc2 > R(0)) vort_ad = vort_ad - (rs * sk2[i]) * ldv<V>(in.tu + oe);
+      if (ph.visc4 > R(0)) vort_ad = vort_ad - rs * ldv<V>(w.du_ad + oe);
+    } else {
+      pvv_ad = pvv_ad + sg * (gpt_ad / dve);
+      if (ph.visc2 > R(0)) {
+        const M ud2 = sk2[i] * ldv<V>(in.tu + oe);
+        vort_ad = vort_ad + (-sg) * (ud2 / dve);
+      }
+      if (ph.visc4 > R(0)) vort_ad = vort_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dve);
     }
-    if (ph.visc4 > R(0)) vort_ad = vort_ad + (-sg) * (ldv<V>(w.du_ad + oe) / dve);
   }
   const R hv = ld(bs.hv, v), area = ld(m.v_area, v);
   M hv_ad = mv_fill<R, V>(sd.hv ? sd.hv[v] : R(0));
