@@ -347,16 +347,25 @@ __global__ void k_tl_vertex_st(MeshDev<R> m, int B, Base<R> bs, const R *__restr
     circ = circ + ssg[i] * (sdc[i] * ldv<V>(ut + (size_t)se[i] * B + b));
   }
   const R area = ld(m.v_area, v);
-  const M vort = circ / area;
   M hvt = mv_fill<R, V>(R(0));
 #pragma unroll
   for (int k = 0; k < VDEG; k++) {
     const int i = k * vpb + lv;
     hvt = hvt + ldv<V>(ht + (size_t)sc[i] * B + b) * skt[i];
   }
-  hvt = hvt / area;
   const R hv = ld(bs.hv, v);
-  const M pvt = vort / hv - (hvt * (ld(m.v_f, v) + ld(bs.vort, v))) / (hv * hv);
+  M vort, pvt;
+  if constexpr (sizeof(R) == 4) {
+    // FP32 members: reciprocals of areaTriangle and h_vertex formed once per vertex
+    const R ra = R(1) / area, rh = R(1) / hv;
+    vort = circ * ra;
+    hvt = hvt * ra;
+    pvt = vort * rh - hvt * (((ld(m.v_f, v) + ld(bs.vort, v)) * rh) * rh);
+  } else {
+    vort = circ / area;
+    hvt = hvt / area;
+    pvt = vort / hv - (hvt * (ld(m.v_f, v) + ld(bs.vort, v))) / (hv * hv);
+  }
   const size_t o = (size_t)v * B + b;
   if (d.circ) stv<V>(d.circ + o, circ);
   stv<V>(d.vort + o, vort);
@@ -489,16 +498,30 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
       ke = ke + sr[4 * SC + i] * (sr[5 * SC + i] * ldv<V>(ut + (size_t)si[2 * SC + i] * B + b));
     }
   }
-  ke = ke / area;
   M pc = mv_fill<R, V>(R(0)), vc = mv_fill<R, V>(R(0));
-  MPSW_SLOTS(k, S, S) {
-    const int i = k * cpb + lc;
-    const int v = si[3 * SC + i];
-    const R kt = sr[6 * SC + i];
-    pc = pc + (kt * ldv<V>(d.pvv + (size_t)v * B + b)) / area;
-    if (d.vc) vc = vc + (kt * ldv<V>(d.vort + (size_t)v * B + b)) / area;
+  if constexpr (sizeof(R) == 4) {
+    // FP32 members: 1 / areaCell formed once, no division per member
+    const R ra = R(1) / area;
+    ke = ke * ra;
+    MPSW_SLOTS(k, S, S) {
+      const int i = k * cpb + lc;
+      const int v = si[3 * SC + i];
+      const R kr = sr[6 * SC + i] * ra;
+      pc = pc + kr * ldv<V>(d.pvv + (size_t)v * B + b);
+      if (d.vc) vc = vc + kr * ldv<V>(d.vort + (size_t)v * B + b);
+    }
+    th = th * ra;
+  } else {
+    ke = ke / area;
+    MPSW_SLOTS(k, S, S) {
+      const int i = k * cpb + lc;
+      const int v = si[3 * SC + i];
+      const R kt = sr[6 * SC + i];
+      pc = pc + (kt * ldv<V>(d.pvv + (size_t)v * B + b)) / area;
+      if (d.vc) vc = vc + (kt * ldv<V>(d.vort + (size_t)v * B + b)) / area;
+    }
+    th = th / area;
   }
-  th = th / area;
   const size_t o = (size_t)c * B + b;
   stv<V>(d.div + o, div);
   stv<V>(d.ke + o, ke);
@@ -522,14 +545,16 @@ __device__ __forceinline__ void tl_edge_diag_body(const MeshDev<R> &m, int B, co
   const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
   const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
   const M pv1 = ldv<V>(d.pvv + (size_t)v1 * B + b), pv2 = ldv<V>(d.pvv + (size_t)v2 * B + b);
-  const M gptt = (pv2 - pv1) / dv;
+  // FP32 members: multiply by 1 / dvEdge, 1 / dcEdge instead of dividing each member
+  const M gptt = sizeof(R) == 4 ? (pv2 - pv1) * (R(1) / dv) : (pv2 - pv1) / dv;
   // pv_edge's two vertex terms: the reference adds them over edgesOnVertex, which lists the same
   // two endpoints; a sum of two terms is the same in either order, so the loaded rows serve
   M pet = mv_fill<R, V>(R(0));
   pet = pet + R(0.5) * pv1;
   pet = pet + R(0.5) * pv2;
   pet = pet - ((ph.apvm * vt) * ph.dt) * ld(bs.gpt, e) - ((ph.apvm * ld(bs.v, e)) * ph.dt) * gptt;
-  const M gpnt = (ldv<V>(d.pc + (size_t)c2 * B + b) - ldv<V>(d.pc + (size_t)c1 * B + b)) / dc;
+  const M dpc = ldv<V>(d.pc + (size_t)c2 * B + b) - ldv<V>(d.pc + (size_t)c1 * B + b);
+  const M gpnt = sizeof(R) == 4 ? dpc * (R(1) / dc) : dpc / dc;
   const M uet = ldv<V>(ut + (size_t)e * B + b);
   pet = pet - ((ph.apvm * uet) * ph.dt) * ld(bs.gpn, e) - ((ph.apvm * ld(bs.u, e)) * ph.dt) * gpnt;
   const size_t o = (size_t)e * B + b;
@@ -612,8 +637,10 @@ __device__ __forceinline__ void tl_edge_tend_body(const MeshDev<R> &m, int B, co
   }
   const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
   const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
-  M tut = qt - ((ldv<V>(d.ke + (size_t)c2 * B + b) - ldv<V>(d.ke + (size_t)c1 * B + b)) +
-                R(GRAVITY) * (ldv<V>(ht + (size_t)c2 * B + b) - ldv<V>(ht + (size_t)c1 * B + b))) / dc;
+  const M grad = (ldv<V>(d.ke + (size_t)c2 * B + b) - ldv<V>(d.ke + (size_t)c1 * B + b)) +
+                 R(GRAVITY) * (ldv<V>(ht + (size_t)c2 * B + b) - ldv<V>(ht + (size_t)c1 * B + b));
+  // FP32 members: multiply by 1 / dcEdge instead of dividing each member
+  M tut = sizeof(R) == 4 ? qt - grad * (R(1) / dc) : qt - grad / dc;
   if (ph.visc2 > R(0)) {
     M ud = (ldv<V>(d.div + (size_t)c2 * B + b) - ldv<V>(d.div + (size_t)c1 * B + b)) / dc -
            (ldv<V>(d.vort + (size_t)v2 * B + b) - ldv<V>(d.vort + (size_t)v1 * B + b)) / dv;
@@ -1185,7 +1212,12 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
   if (tn) {
     Mv<R, V> r;
 #pragma unroll
-    for (int i = 0; i < V; i++) r.x[i] = is_edge ? R(next.x[i]) : R(next.x[i] / A(area));
+    for (int i = 0; i < V; i++) {
+      if constexpr (sizeof(R) == 4)  // FP32 members: one reciprocal of areaCell per cell
+        r.x[i] = is_edge ? R(next.x[i]) : R(next.x[i] * (A(1) / A(area)));
+      else
+        r.x[i] = is_edge ? R(next.x[i]) : R(next.x[i] / A(area));
+    }
     stv<V>(tn + o, r);
   }
 }
