@@ -19,6 +19,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -185,7 +186,9 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, 'gpurun_out', 'clocks_%d.csv' % os.getpid())
+        # the raw samples; MPSW_CLOCKS_DIR keeps them somewhere chosen by the caller
+        out = os.environ.get('MPSW_CLOCKS_DIR') or tempfile.gettempdir()
+        self.path = os.path.join(out, 'mpsw_clocks_%d.csv' % os.getpid())
 
     def __enter__(self):
         try:

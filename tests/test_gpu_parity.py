@@ -3,7 +3,7 @@ on identical inputs, through the drop-in module surface.
 
 Tolerances (relative to the field's max magnitude): forward and tangent-linear steps are
 computed with the reference's operation order and no FMA, so they are held to 1e-13 per step
-(the north-star bar is 1e-12 after one step); the adjoint gathers sum in a different order
+(the bar for the FP64 path is 1e-12 after one step); the adjoint gathers sum in a different order
 than the reference's reverse scatters, so it is held to 1e-11.
 """
 import numpy as np

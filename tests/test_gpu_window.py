@@ -1,7 +1,7 @@
 """Batched device-resident windows (B members on the trailing dimension) and the autograd
 step: FP64 windows agree with the single-member module path, the FP64 window's tangent linear
 and adjoint pass the dot-product test, and the FP32-stencil / FP64-accumulation windows stay
-within 1e-4 relative L2 error of the FP64 window."""
+within 1e-4 relative L2 error of the FP64 window (the bar for the FP32-stencil form)."""
 import numpy as np
 import pytest
 
