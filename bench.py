@@ -179,6 +179,26 @@ def run_reference(a, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---- host jitter ----------------------------------------------------------------------------------
+class host_quiet:
+    """Python's cyclic garbage collector paused over the timed steps (after one collection and
+    with the set-up's objects frozen), so a full collection cannot stall the host thread that
+    feeds the GPU in the middle of a timed step.  close() restores it."""
+
+    def __init__(self):
+        import gc
+        self.gc = gc
+        gc.collect()
+        gc.freeze()
+        self.was = gc.isenabled()
+        gc.disable()
+
+    def close(self):
+        if self.was:
+            self.gc.enable()
+        self.gc.unfreeze()
+
+
 # ---- clocks -------------------------------------------------------------------------------------
 class Clocks:
     FIELDS = 'index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap'
@@ -343,6 +363,7 @@ def run_mpsw(a, rank, world):
             fn()
         times = []
         launches0 = L.mpsw_launch_count()
+        quiet = host_quiet()
         for _ in range(n_time):
             flush.zero_()  # L2 flush between timed iterations, outside the timed region
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -354,6 +375,7 @@ def run_mpsw(a, rank, world):
             torch.cuda.synchronize()
             barrier()
             times.append(e0.elapsed_time(e1))
+        quiet.close()
         return times, (L.mpsw_launch_count() - launches0) / n_time
 
     if world > 1:
@@ -724,6 +746,7 @@ def run_costs(a, rank, world):
             fn()
         times = []
         launches0 = L.mpsw_launch_count()
+        quiet = host_quiet()
         for _ in range(n_time):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -735,6 +758,7 @@ def run_costs(a, rank, world):
             torch.cuda.synchronize()
             barrier()
             times.append(e0.elapsed_time(e1))
+        quiet.close()
         return times, (L.mpsw_launch_count() - launches0) / n_time
 
     with Clocks(dev) as clk:
