@@ -67,8 +67,9 @@ def test_window_ad_matches_module_adj():
         assert rel(rh[:, b].cpu().numpy(), m.h_ad[0, 0]) < 1e-13
 
 
-def test_window_dot_product_and_fp32():
-    m, e = engine(level=4, dt=300.0)
+@pytest.mark.parametrize('cfg', [dict(), dict(visc2=1e5, visc4=5e14, drag=True, wind=True)])
+def test_window_dot_product_and_fp32(cfg):
+    m, e = engine(level=4, dt=300.0, **cfg)
     nsteps, B = 24, 4
     du, dh = members(m, B, 3)
     w = e.window(nsteps, ckpt_every=5)
