@@ -161,7 +161,8 @@ def run_reference(a, rank, world):
     vals = []
     with mp.get_context('spawn').Pool(workers) as pool:
         for i in range(a.warmup + a.steps):
-            sec, wall, per = cpu_gradient_seconds(a.level, a.dt, a.nsteps, 1 if i == 0 else sample,
+            # warm-up steps run one-step samples (they only start the processes and warm caches)
+            sec, wall, per = cpu_gradient_seconds(a.level, a.dt, a.nsteps, 1 if i < a.warmup else sample,
                                                   workers, pool)
             if i >= a.warmup:
                 vals.append(workers / sec)
