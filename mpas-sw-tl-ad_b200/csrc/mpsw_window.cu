@@ -445,7 +445,6 @@ template <typename R>
 static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, MemberBufs<R> *mb,
                             const Phys<R> &ph, const double w[4], const double c[4], int k, const Base<R> &bs,
                             cudaStream_t st, bool round_in) {
-  Window &W = E.win;
   const MeshDev<R> &m = mesh_for<R>(E);
   const R *uti = k == 0 ? nullptr : mb->pu[k - 1];
   const R *hti = k == 0 ? nullptr : mb->ph[k - 1];
