@@ -5,7 +5,6 @@ within 1e-4 relative L2 error of the FP64 window (the bar for the FP32-stencil f
 import numpy as np
 import pytest
 
-import oracle as O
 from helpers import rel, setup
 from module_sw_mpas import MpasSwModule
 

@@ -1,7 +1,6 @@
 """Replica parallelism host logic (mpsw/replicas.py) on CPU with the gloo backend, world size 2:
 shards cover every member exactly once, the job time is the slowest rank's, and gathered
 members come back in member order on every rank."""
-import os
 import socket
 
 import pytest
