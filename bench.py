@@ -1,8 +1,8 @@
 """Benchmark: tangent-linear + adjoint gradients per second of the MPAS shallow-water RK4 model.
 
-Workload (default): level-5 bisected-icosahedron TRiSK mesh (10242 cells, 30720 edges, 20480
-vertices), seeded balanced flow (seed 0), dt = 300 s, a 288-step (24 h) window, trajectory
-checkpointed every 16 steps, perturbations h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s).  One bench step
+Workload (default): level-7 bisected-icosahedron TRiSK mesh (163842 cells, 491520 edges, 327680
+vertices), seeded balanced flow (seed 0), dt = 75 s, a 288-step (6 h) window, trajectory
+checkpointed every 16 steps, perturbations h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s), B = 64 members.  One bench step
 is one gradient batch: the nonlinear window with checkpoints, the B-member tangent-linear
 sweep and the B-member adjoint sweep (seeded with the tangent-linear output, i.e. the gradient
 of 1/2 |L dx|^2).  `value` counts gradients of the batched FP32-stencil / FP64-accumulation
@@ -39,7 +39,7 @@ def parse():
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='mpsw', choices=['mpsw', 'reference'])
     p.add_argument('--workload', default='tlad', choices=['tlad', 'fwd', 'costs'],
-                   help='tlad: batched TL+AD gradients (level 5, 288 steps of 300 s, B=64); '
+                   help='tlad: batched TL+AD gradients (level 7, 288 steps of 75 s, B=64); '
                         'fwd: nonlinear forward with mountains (level 7, 1152 steps of 75 s), sim-days/s; '
                         'costs: 64 cost-function gradients by one batched adjoint (level 6, 1152 steps of 150 s)')
     p.add_argument('--batch', type=int, default=64)
@@ -56,7 +56,7 @@ def parse():
     p.add_argument('--profile', action='store_true',
                    help='only the timed batched windows (for profiler launch lists); no JSON line')
     a = p.parse_args()
-    dflt = {'tlad': (5, 288, 300.0), 'fwd': (7, 1152, 75.0), 'costs': (6, 1152, 150.0)}[a.workload]
+    dflt = {'tlad': (7, 288, 75.0), 'fwd': (7, 1152, 75.0), 'costs': (6, 1152, 150.0)}[a.workload]
     a.level = dflt[0] if a.level is None else a.level
     a.nsteps = dflt[1] if a.nsteps is None else a.nsteps
     a.dt = dflt[2] if a.dt is None else a.dt
@@ -105,79 +105,157 @@ def perturbations(unit, B, seed=1):
 
 
 # ---- reference arm and CPU baseline: the oracle (serial C restatement of the Fortran) -------
-def _oracle_sample(args):
-    """Time `n` forward, tangent-linear and adjoint steps of one member on the host."""
-    level, dt, n, seed = args
-    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    import numpy as np
-    import oracle as O
-    unit, mesh, st = workload(level, dt)
-    m = O.OracleModule()
-    load_module(m, unit, mesh, st, dt)
-    m.var_allocation_tlm()
-    m.var_allocation_adj()
-    m.sw_mpas_init_block()
-    dh, du = perturbations(unit, 1, seed)
-    m.u_tl[0, 0], m.h_tl[0, 0] = du[:, 0], dh[:, 0]
-    u0, h0 = m.u[0, 0].copy(), m.h[0, 0].copy()
-    t0 = time.perf_counter()
-    for _ in range(n):
-        m.sw_rk4()
-    t1 = time.perf_counter()
-    m.u[0, 0], m.h[0, 0] = u0, h0
-    for _ in range(n):
-        m.sw_rk4_tlm()
-    t2 = time.perf_counter()
-    m.u_ad[0, 0], m.h_ad[0, 0] = m.u_tl[0, 0], m.h_tl[0, 0]
-    for _ in range(n):
-        m.u[0, 0], m.h[0, 0] = u0, h0
-        m.sw_rk4_adj()
-    t3 = time.perf_counter()
-    return (t1 - t0) / n, (t2 - t1) / n, (t3 - t2) / n
+class OracleMember:
+    """One member's oracle instance on the host: the workload's mesh, balanced flow and a seeded
+    perturbation, built once; sample(n) times n forward, n tangent-linear and n adjoint steps."""
+
+    def __init__(self, level, dt, seed):
+        sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+        import oracle as O
+        unit, mesh, st = workload(level, dt)
+        m = O.OracleModule()
+        load_module(m, unit, mesh, st, dt)
+        m.var_allocation_tlm()
+        m.var_allocation_adj()
+        m.sw_mpas_init_block()
+        dh, du = perturbations(unit, 1, seed)
+        self.m, self.du, self.dh = m, du[:, 0].copy(), dh[:, 0].copy()
+        self.u0, self.h0 = m.u[0, 0].copy(), m.h[0, 0].copy()
+
+    def sample(self, n):
+        """Seconds per step of the forward, tangent-linear and adjoint sweeps (n steps each)."""
+        m = self.m
+        m.u[0, 0], m.h[0, 0] = self.u0, self.h0
+        m.u_tl[0, 0], m.h_tl[0, 0] = self.du, self.dh
+        t0 = time.perf_counter()
+        for _ in range(n):
+            m.sw_rk4()
+        t1 = time.perf_counter()
+        m.u[0, 0], m.h[0, 0] = self.u0, self.h0
+        for _ in range(n):
+            m.sw_rk4_tlm()
+        t2 = time.perf_counter()
+        m.u_ad[0, 0], m.h_ad[0, 0] = m.u_tl[0, 0], m.h_tl[0, 0]
+        for _ in range(n):
+            m.u[0, 0], m.h[0, 0] = self.u0, self.h0
+            m.sw_rk4_adj()
+        t3 = time.perf_counter()
+        return (t1 - t0) / n, (t2 - t1) / n, (t3 - t2) / n
 
 
-def cpu_gradient_seconds(level, dt, nsteps, sample_steps, workers, pool=None):
-    """Seconds per gradient of the serial reference restatement, from a bounded sample on each
-    of `workers` host processes run concurrently (the slowest process's per-step time,
-    extrapolated linearly to the full window: one forward with trajectory, one TL and one AD
-    sweep)."""
-    t0 = time.perf_counter()
-    if workers == 1 or pool is None:
-        per = [_oracle_sample((level, dt, sample_steps, 1))]
-    else:
-        per = pool.map(_oracle_sample, [(level, dt, sample_steps, 1 + i) for i in range(workers)])
-    wall = time.perf_counter() - t0
-    step_s = max(f + t + a for f, t, a in per)
-    return step_s * nsteps, wall, per
+def _oracle_worker(conn, level, dt, seed):
+    """Host process of the reference arm: builds its member once, then runs one sample per
+    request (n steps of each sweep) and answers with the per-step seconds."""
+    try:
+        om = OracleMember(level, dt, seed)
+        conn.send('ready')
+        while True:
+            n = conn.recv()
+            if n is None:
+                break
+            conn.send(om.sample(n))
+    except Exception as e:  # reported to the parent, which raises
+        conn.send('error: %r' % (e,))
+
+
+class OracleWorkers:
+    """`count` host processes (spawned, before any GPU use), each with its own member; one
+    bench step sends every process one sample request at once and waits for all answers."""
+
+    def __init__(self, count, level, dt):
+        import multiprocessing as mp
+        ctx = mp.get_context('spawn')
+        self.procs, self.conns = [], []
+        for i in range(count):
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_oracle_worker, args=(b, level, dt, 1 + i), daemon=True)
+            p.start()
+            self.procs.append(p)
+            self.conns.append(a)
+        for c in self.conns:
+            r = c.recv()
+            if r != 'ready':
+                raise RuntimeError('oracle worker failed: %s' % r)
+
+    def step(self, n):
+        """One sample on every process at once: (wall seconds, per-process per-step seconds)."""
+        t0 = time.perf_counter()
+        for c in self.conns:
+            c.send(n)
+        per = [c.recv() for c in self.conns]
+        wall = time.perf_counter() - t0
+        bad = [r for r in per if isinstance(r, str)]
+        if bad:
+            raise RuntimeError('oracle worker failed: %s' % bad[0])
+        return wall, per
+
+    def close(self):
+        for c in self.conns:
+            try:
+                c.send(None)
+            except Exception:
+                pass
+        for p in self.procs:
+            p.join(timeout=10)
 
 
 def run_reference(a, rank, world):
-    # rank 0 alone times the host baseline; other ranks exit without work
-    if rank != 0:
+    """The reference's CPU path (the serial oracle, one member per host process on every host
+    core at once).  One bench step is one sample: each process runs one forward, one
+    tangent-linear and one adjoint step of its member; `ms_per_step` is that sample's wall time
+    and `value` the gradients per second it implies for the full window (linear in steps)."""
+    if rank != 0:  # rank 0 alone times the host baseline; other ranks exit without work
         return
-    import multiprocessing as mp
     workers = os.cpu_count() or 1
-    sample = max(2, min(12, a.nsteps))
-    vals = []
-    with mp.get_context('spawn').Pool(workers) as pool:
-        for i in range(a.warmup + a.steps):
-            # warm-up steps run one-step samples (they only start the processes and warm caches)
-            sec, wall, per = cpu_gradient_seconds(a.level, a.dt, a.nsteps, 1 if i < a.warmup else sample,
-                                                  workers, pool)
-            if i >= a.warmup:
-                vals.append(workers / sec)
-    v = statistics.median(vals)
+    pool = OracleWorkers(workers, a.level, a.dt)
+    try:
+        for _ in range(a.warmup):
+            pool.step(1)
+        walls, grads = [], []
+        for _ in range(a.steps):
+            wall, per = pool.step(1)
+            walls.append(wall)
+            step_s = max(f + t + d for f, t, d in per)  # the slowest process's fwd + TL + AD step
+            grads.append(workers / (step_s * a.nsteps))
+    finally:
+        pool.close()
+    v = statistics.median(grads)
+    ms = 1e3 * statistics.mean(walls)
     line = {
         'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': a.gpus,
-        'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': 1e3 * workers / v,
+        'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': ms,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh)' % a.level,
-        'config': {'workload': 'TL+AD window, level %d mesh, %d steps of %g s, 1 member per host process' % (a.level, a.nsteps, a.dt)},
+        'config': workload_config(a),
+        'sample_ms': [round(1e3 * w, 1) for w in walls],
+        'extrapolation': {'steps_per_sample': 1, 'window_steps': a.nsteps,
+                          'seconds_per_gradient_per_process': workers / v,
+                          'note': 'value = processes / (slowest process fwd+TL+AD step seconds x window steps)'},
         'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': workers, 'kind': 'port',
-                         'sample': '%d forward + %d TL + %d AD steps per process, extrapolated to %d steps' % (sample, sample, sample, a.nsteps)},
+                         'sample': '1 forward + 1 TL + 1 AD step per process on %d processes, extrapolated to %d steps' % (workers, a.nsteps)},
         'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_gradient_seconds(level, dt, nsteps, target_s=15.0):
+    """Seconds per gradient of the serial reference restatement on one host core, from a bounded
+    sample (about target_s seconds of host work) extrapolated to the window; and the sample's
+    step count."""
+    om = OracleMember(level, dt, 1)
+    f, t, d = om.sample(1)
+    n = max(1, min(30, int(target_s / max(f + t + d, 1e-6)) - 1))
+    f, t, d = om.sample(n)
+    return (f + t + d) * nsteps, n
+
+
+def workload_config(a):
+    """`config` of the TL+AD bench line (both arms)."""
+    nC = 10 * 4 ** a.level + 2
+    return {'workload': 'TL+AD window: level-%d mesh (%d cells), %d RK4 steps of %g s, %d members, checkpoint every %d'
+                        % (a.level, nC, a.nsteps, a.dt, a.batch, a.ckpt),
+            'members_per_gpu': a.batch, 'parallelism': 'replicas x%d' % a.gpus,
+            'l2': 'GPU arm: flushed (256 MB write) between timed steps; working set far above L2'}
 
 
 # ---- host jitter ----------------------------------------------------------------------------------
@@ -432,12 +510,17 @@ def run_mpsw(a, rank, world):
     out_u = torch.empty_like(du_host).pin_memory()
     out_h = torch.empty_like(dh_host).pin_memory()
 
+    # device buffers of the public-API path, allocated once: a step allocates nothing
+    xu, xh = torch.empty_like(du), torch.empty_like(dh)
+    work = (torch.empty_like(du), torch.empty_like(dh))
+    res = (torch.empty_like(du), torch.empty_like(dh))
+
     def e2e_step():
         w = Window(eng, a.nsteps, a.ckpt, a.storage)
-        xu = du_host.to('cuda', non_blocking=True)
-        xh = dh_host.to('cuda', non_blocking=True)
-        tu, th = w.tl(xu, xh, FP32)
-        gu, gh = w.ad(tu, th, FP32)
+        xu.copy_(du_host, non_blocking=True)
+        xh.copy_(dh_host, non_blocking=True)
+        tu, th = w.tl(xu, xh, FP32, work=work, out=res)
+        gu, gh = w.ad(tu, th, FP32, work=work, out=(xu, xh))
         out_u.copy_(gu, non_blocking=True)
         out_h.copy_(gh, non_blocking=True)
 
@@ -480,8 +563,7 @@ def run_mpsw(a, rank, world):
     # host baseline: serial oracle on one core, bounded sample
     cpu = None
     if rank == 0:
-        sample = 30
-        sec, wall, per = cpu_gradient_seconds(a.level, a.dt, a.nsteps, sample, 1)
+        sec, sample = cpu_gradient_seconds(a.level, a.dt, a.nsteps)
         cpu = {'value': 1.0 / sec, 'unit': UNIT, 'cores': 1, 'kind': 'port',
                'sample': '%d forward + %d TL + %d AD steps of one member, extrapolated to %d steps' % (sample, sample, sample, a.nsteps)}
 
@@ -492,10 +574,9 @@ def run_mpsw(a, rank, world):
             'warmup': a.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f32 stencils + f64 accumulation',
             'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh, seeded perturbations)' % a.level,
-            'config': {'workload': 'TL+AD window: level-%d mesh (%d cells), %d RK4 steps of %g s, %d members, checkpoint every %d' % (a.level, nC, a.nsteps, a.dt, B, a.ckpt),
-                       'stage_storage': {-1: 'auto (FP64+FP32 stage linearisation points when they fit 40%% of free HBM)', 0: 'none: stages recomputed from checkpoints', 1: 'FP64', 2: 'FP32', 3: 'FP64+FP32'}[a.storage],
-                       'members_per_gpu': B, 'parallelism': 'replicas x%d' % world,
-                       'l2': 'flushed (256 MB write) between timed steps; working set ~%.0f MB' % wset},
+            'config': workload_config(a),
+            'stage_storage': {-1: 'auto (FP64+FP32 stage linearisation points when they fit 40%% of free HBM)', 0: 'none: stages recomputed from checkpoints', 1: 'FP64', 2: 'FP32', 3: 'FP64+FP32'}[a.storage],
+            'working_set_mb': round(wset),
             'step_ms': [round(t, 3) for t in t32],
             'phase_ms': phases,
             'fp64_plain_gradients_per_s': plain,
@@ -817,8 +898,28 @@ def run_costs(a, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(n):
+    """`bench.py --gpus N` started without a launcher: start N rank processes of this script (one
+    per GPU, as torchrun would: RANK, LOCAL_RANK, WORLD_SIZE, MASTER_ADDR/PORT set), pass rank 0's
+    output through, and return the first nonzero exit status (0 when all succeed)."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(('127.0.0.1', 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env=env,
+                                      stdout=None if r == 0 else subprocess.DEVNULL))
+    rcs = [p.wait() for p in procs]
+    return next((rc for rc in rcs if rc), 0)
+
+
 def main():
     a = parse()
+    if 'WORLD_SIZE' not in os.environ and a.gpus > 1 and a.impl == 'mpsw':
+        sys.exit(spawn_ranks(a.gpus))
     rank = int(os.environ.get('RANK', '0'))
     world = int(os.environ.get('WORLD_SIZE', '1'))
     if world > 1:

@@ -160,10 +160,13 @@ int mpsw_grid_to_points(mpsw_handle *h, int nlat, int nlon, const double *lat1d,
  * the mesh must need at most 2,097,152 doubles of scratch, 3*nVertices + 3*nCells +
  * 2*nEdges (plus nEdges + nVertices + nCells with del4 viscosity), i.e. up to about 140,000
  * cells (100,000 with del4) on a quasi-uniform mesh; larger meshes are refused with
- * MPSW_ERR_UNSUPPORTED.  On success the call allocates
- * nothing; the first call on each device looks up the array's address (make that first call
- * before any stream capture).  Every call on a device shares the array, so calls whose work
- * overlaps on the GPU (other streams, other threads, other handles) race; order them. */
+ * MPSW_ERR_UNSUPPORTED.  The call allocates nothing: sw_mpas_init_block, when it puts the
+ * mesh on a device, also looks up the array's address there and loads the array and the
+ * kernels this call launches (which lazy module loading, the CUDA default, would otherwise do
+ * at the first call), so run that set-up before the device's memory is reserved.  The current
+ * device must be the one the handle's mesh was built on (else MPSW_ERR_STATE).  Every call on a
+ * device shares the array, so calls whose work overlaps on the GPU (other streams, other
+ * threads, other handles) race; order them. */
 int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const double *hh, double *tend_u,
                               double *tend_h, void *stream);
 
@@ -173,11 +176,11 @@ int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const double *hh,
 int mpsw_get_stream(mpsw_handle *h, void **stream);
 /* Number of kernels the library has launched in this process (all handles). */
 long long mpsw_launch_count(void);
-/* Average time of `iters` back-to-back launches of one member stencil kernel on the buffers
- * of the last window sweep (same precision and B): which = 0 tl_vertex, 1 tl_cell,
- * 2 tl_edge_diag, 3 tl_edge_tend, 4 ad_edge, 5 ad_cell, 6 ad_vertex, 7 ad_final; or of a whole
- * stage: 8 tangent-linear stage, 9 adjoint stage.  Timed with CUDA events on the engine's
- * stream. */
+/* Average time of `iters` launches of one member stencil kernel on the buffers of the last
+ * window sweep (same precision and B): which = 0 tl_vertex, 1 tl_cell, 2 tl_edge_diag,
+ * 3 tl_edge_tend, 4 ad_edge, 5 ad_cell, 6 ad_vertex, 7 ad_final; or of a whole stage:
+ * 8 tangent-linear stage, 9 adjoint stage.  Each launch is timed alone with CUDA events on the
+ * engine's stream, after a 256 MiB write that evicts L2 (a cold start, as in a sweep). */
 int mpsw_time_kernel(mpsw_handle *h, int which, int precision, int B, int iters, double *ms_per_launch);
 
 #ifdef __cplusplus

@@ -207,10 +207,16 @@ Engine::~Engine() {
   for (void *p : work) cudaFree(p);
   if (trc) cudaFree(trc);
   window_free();
+  if (l2_flush) cudaFree(l2_flush);
   for (cudaEvent_t ev : {ev_fork, ev_step, ev_join})
     if (ev) cudaEventDestroy(ev);
   if (side) cudaStreamDestroy(side);
   if (stream) cudaStreamDestroy(stream);
+}
+
+void *Engine::l2_flush_buffer() {
+  if (!l2_flush) cuda_check(cudaMalloc(&l2_flush, kL2Flush), "cudaMalloc L2 flush buffer");
+  return l2_flush;
 }
 
 void *Engine::dalloc(size_t bytes) {
@@ -463,6 +469,8 @@ void Engine::build_device_mesh() {
   d_perm[0] = up<int>(bm.perm_c, mesh_bufs);
   d_perm[1] = up<int>(bm.perm_e, mesh_bufs);
   d_perm[2] = up<int>(bm.perm_v, mesh_bufs);
+  cuda_check(cudaGetDevice(&mesh_device), "cudaGetDevice");
+  noalloc_prepare_device();
   mesh_built = true;
   mesh_dirty = false;
   for (auto &v : vars)

@@ -118,6 +118,7 @@ struct Engine {
   std::vector<void *> mesh_bufs;
   const int *d_perm[3] = {nullptr, nullptr, nullptr};
   const int *d_cnb = nullptr;  // [MAXE][nCells] the cell across each edge of a cell
+  int mesh_device = -1;        // the CUDA device the mesh (and everything derived) lives on
 
   // work
   std::vector<void *> work;
@@ -134,6 +135,10 @@ struct Engine {
   long long trc_n = 0;
   int pending_diag = 0;  // 1: diagnostics of the level-1 state owed, 2: and their tangents
   Phys<double> phys_cache{};  // physics scalars, refreshed whenever a scalar is assigned
+  // buffer larger than L2 that kernel timing writes between launches (allocated on first use)
+  static constexpr size_t kL2Flush = (size_t)256 << 20;
+  void *l2_flush = nullptr;
+  void *l2_flush_buffer();
   void refresh_phys();
   Window win;
 
@@ -277,6 +282,11 @@ struct mpsw_handle {
 };
 
 namespace mpsw {
+// Prepares the current device for mpsw_compute_tend_noalloc (mpsw_noalloc.cu): looks up the
+// address of its scratch array and loads the kernels it launches, so that the entry point
+// itself allocates and loads nothing.
+void noalloc_prepare_device();
+
 // Runs f on the handle's engine, turning exceptions into status codes (none cross the ABI).
 template <typename F>
 int guarded(mpsw_handle *h, F &&f) {

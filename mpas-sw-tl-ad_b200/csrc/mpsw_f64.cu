@@ -8,13 +8,6 @@ long long g_launches = 0;
 thread_local const TuneTable *g_tune = nullptr;
 thread_local bool g_stable_base = false;
 
-int grid_for(long long total) {
-  long long g = (total + kThreads - 1) / kThreads;
-  const long long cap = 148LL * 16;  // 16 resident 256-thread blocks on each of the 148 SMs
-  if (g < 1) g = 1;
-  return (int)(g < cap ? g : cap);
-}
-
 void convert_d2f(long long n, const double *src, float *dst, cudaStream_t s) {
   g_launches++;
   launch_k(k_convert<double, float>, launch_cfg(n), s, n, src, dst);

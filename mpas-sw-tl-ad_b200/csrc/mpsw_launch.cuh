@@ -131,6 +131,17 @@ constexpr int kWideV = sizeof(R) == 4 ? 8 : 0;
     __VA_ARGS__;                                                \
   }
 
+// run the statement once with NB = BoundsNarrow and once with NB = BoundsAny
+#define MPSW_BDISPATCH_ALL(...)  \
+  {                              \
+    using NB = BoundsNarrow;     \
+    __VA_ARGS__;                 \
+  }                              \
+  {                              \
+    using NB = BoundsAny;        \
+    __VA_ARGS__;                 \
+  }
+
 #define MPSW_VDISPATCH(v, ...)                            \
   switch (v) {                                            \
     case 8: { constexpr int VV = 8; if constexpr (sizeof(R) == 4) { __VA_ARGS__; } } break; \
@@ -181,6 +192,19 @@ void Launch<R, A>::tracer_stage(const MeshDev<R> &m, const int *c_nb, int nT, co
   g_launches++;
   MPSW_BDISPATCH(m, launch_k(k_tracer_stage<R, NB::c>, launch_cfg((long long)nT * m.nC), s, m, c_nb, nT, u, he, tr_in,
                              tr0, h0, h_next, tend, acc, tr_next, c, w, first, last));
+}
+template <typename R, typename A>
+cudaError_t Launch<R, A>::preload_forward() {
+  cudaFuncAttributes fa;
+  cudaError_t err = cudaSuccess;
+  auto load = [&](const void *k) {
+    const cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (err == cudaSuccess) err = e;
+  };
+  load((const void *)k_fwd_vertex<R>);
+  MPSW_BDISPATCH_ALL(load((const void *)k_fwd_cell<R, A, NB::c>); load((const void *)k_fwd_edge_diag<R, NB::e2>);
+                     load((const void *)k_fwd_edge_tend<R, A, NB::e2>); load((const void *)k_del4_vc<R, 1, NB>));
+  return err;
 }
 template <typename R, typename A>
 void Launch<R, A>::tend_h(const MeshDev<R> &m, const R *u, const R *he, R *out, cudaStream_t s) {

@@ -9,7 +9,6 @@
 
 namespace mpsw {
 
-int grid_for(long long total);
 extern long long g_launches;
 
 // Launch choices of the member kernels, picked per (precision, B) by the window's autotuner:
@@ -60,6 +59,9 @@ struct Launch {
                            int last, cudaStream_t s);
   static void recon(const MeshDev<R> &m, int B, int sphere, const R *u, R *X, R *Y, R *Z, R *Zon,
                     R *Mer, cudaStream_t s);
+  // load the single-trajectory stage kernels (fwd_vertex .. fwd_edge_tend, del4_vc) onto the
+  // current device now, instead of at their first launch (lazy module loading)
+  static cudaError_t preload_forward();
   // tangent linear, B members
   static void tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut, const R *ht,
                         const Diag<R> &d, cudaStream_t s);

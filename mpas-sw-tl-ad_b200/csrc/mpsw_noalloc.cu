@@ -12,7 +12,11 @@
 // The array below is file-scope device memory: every GPU that loads the library holds its
 // kNoAllocScratchDoubles doubles (16 MiB) until the process exits.  Its name is only a
 // host-side stand-in in host code, so the device address is looked up once per device with
-// cudaGetSymbolAddress (with that device current) and passed to the kernels.
+// cudaGetSymbolAddress (with that device current) and passed to the kernels.  With lazy module
+// loading (the CUDA default) that lookup is what loads the array onto the device, so the engine
+// does it while it builds its mesh on a device (noalloc_prepare_device, called from
+// sw_mpas_init_block), together with loading the kernels the entry point launches: the
+// entry point itself then neither allocates nor loads anything.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -49,6 +53,12 @@ double *scratch_on_current_device() {
 }
 
 }  // namespace
+
+void noalloc_prepare_device() {
+  (void)scratch_on_current_device();
+  cuda_check(Launch<double, double>::preload_forward(), "loading the stage kernels");
+}
+
 }  // namespace mpsw
 
 extern "C" int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const double *hh, double *tend_u,
@@ -58,6 +68,11 @@ extern "C" int mpsw_compute_tend_noalloc(mpsw_handle *h, const double *u, const 
     if (!u || !hh || !tend_u || !tend_h) throw EngineError(MPSW_ERR_ARG, "null state or tendency buffer");
     if (!e.mesh_built || e.mesh_dirty)
       throw EngineError(MPSW_ERR_STATE, "mesh not on the device: call sw_mpas_init_block first (this entry point does not build it)");
+    int dev = -1;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev != e.mesh_device)
+      throw EngineError(MPSW_ERR_STATE, "current device " + std::to_string(dev) + " is not the device " +
+                                            std::to_string(e.mesh_device) + " that holds this handle's mesh");
     const Phys<double> ph = e.phys();
     const size_t nC = (size_t)e.nC, nE = (size_t)e.nE, nV = (size_t)e.nV;
     // diagnostics kept: vorticity, h_vertex, pv_vertex; divergence, ke, pv_cell; pv_edge, h_edge;

@@ -338,14 +338,18 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
   W.nsteps = nsteps;
   W.every = ev;
   W.nckpt = nck;
+  // zero-filled, so the autotuner's first timings (before the forward sweep has written the
+  // stage buffers) read finite values
   auto D = [&](size_t n) {
     void *p = nullptr;
     cuda_check(cudaMalloc(&p, sizeof(double) * n), "cudaMalloc window");
+    cuda_check(cudaMemsetAsync(p, 0, sizeof(double) * n, stream), "memset window");
     return (double *)p;
   };
   auto F = [&](size_t n) {
     void *p = nullptr;
     cuda_check(cudaMalloc(&p, sizeof(float) * n), "cudaMalloc window");
+    cuda_check(cudaMemsetAsync(p, 0, sizeof(float) * n, stream), "memset window");
     return (float *)p;
   };
   for (int i = 0; i < W.nckpt; i++) {
@@ -740,8 +744,11 @@ void Engine::state_to_device(double *u, double *h, cudaStream_t s) {
   join(s, stream, false);
 }
 
+// Average launch time of member kernel `which` (or a whole stage, 8 / 9).  cold: each launch is
+// timed alone, after a write of a buffer larger than L2 (the step's inputs are then read from
+// HBM, as in a sweep over a large mesh); otherwise `iters` launches run back to back.
 template <typename R>
-static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters) {
+static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters, bool cold = false) {
   Window &W = E.win;
   MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
   const MeshDev<R> &m = mesh_for<R>(E);
@@ -790,16 +797,21 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters)
   cudaEvent_t a, b;
   cuda_check(cudaEventCreate(&a), "event");
   cuda_check(cudaEventCreate(&b), "event");
-  cuda_check(cudaEventRecord(a, E.stream), "event");
-  for (int i = 0; i < iters; i++) launch();
-  cuda_check(cudaEventRecord(b, E.stream), "event");
-  cuda_check(cudaEventSynchronize(b), "event");
-  float ms = 0.f;
-  cuda_check(cudaEventElapsedTime(&ms, a, b), "event");
+  double total = 0;
+  for (int rep = 0; rep < (cold ? iters : 1); rep++) {
+    if (cold) cuda_check(cudaMemsetAsync(E.l2_flush_buffer(), rep & 0xff, Engine::kL2Flush, E.stream), "L2 flush");
+    cuda_check(cudaEventRecord(a, E.stream), "event");
+    for (int i = 0; i < (cold ? 1 : iters); i++) launch();
+    cuda_check(cudaEventRecord(b, E.stream), "event");
+    cuda_check(cudaEventSynchronize(b), "event");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, a, b), "event");
+    total += ms;
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   cuda_check(cudaGetLastError(), "time_kernel");
-  return (double)ms / iters;
+  return total / iters;
 }
 
 double Engine::time_kernel(int which, int prec, int B, int iters) {
@@ -807,8 +819,8 @@ double Engine::time_kernel(int which, int prec, int B, int iters) {
   if (which < 0 || which > 9 || B < 1 || iters < 1) throw EngineError(MPSW_ERR_ARG, "bad kernel timing request");
   window_ensure();
   TuneScope scope(tuned_for(prec, B));  // the launch choices the sweeps use
-  return prec == 1 ? time_kernel_impl<float>(*this, which, prec, B, iters)
-                   : time_kernel_impl<double>(*this, which, prec, B, iters);
+  return prec == 1 ? time_kernel_impl<float>(*this, which, prec, B, iters, true)
+                   : time_kernel_impl<double>(*this, which, prec, B, iters, true);
 }
 
 // Autotuner of the member kernels: for each of the eight tangent-linear / adjoint kernels, time

@@ -47,18 +47,22 @@ class Engine:
         self.nE = int(module.nedges)
 
     # ---- layout -------------------------------------------------------------------------
-    def to_internal(self, x: torch.Tensor, kind: int) -> torch.Tensor:
-        n = self.nE if kind == _EDGE else self.nC
-        x = _check_member(x, n, 'input')
-        out = torch.empty_like(x)
-        self.h.call('mpsw_to_internal', kind, x.shape[1], _ptr(x), _ptr(out), _stream())
-        return out
+    def to_internal(self, x: torch.Tensor, kind: int, out: torch.Tensor | None = None) -> torch.Tensor:
+        """x in the reference numbering -> internal order (into `out` when given: a contiguous
+        CUDA float64 tensor of x's shape, so a repeated call allocates nothing)."""
+        return self._permute('mpsw_to_internal', x, kind, out)
 
-    def to_reference(self, x: torch.Tensor, kind: int) -> torch.Tensor:
+    def to_reference(self, x: torch.Tensor, kind: int, out: torch.Tensor | None = None) -> torch.Tensor:
+        return self._permute('mpsw_to_reference', x, kind, out)
+
+    def _permute(self, fn, x, kind, out):
         n = self.nE if kind == _EDGE else self.nC
         x = _check_member(x, n, 'input')
-        out = torch.empty_like(x)
-        self.h.call('mpsw_to_reference', kind, x.shape[1], _ptr(x), _ptr(out), _stream())
+        if out is None:
+            out = torch.empty_like(x)
+        elif out.shape != x.shape or out.dtype != torch.float64 or not out.is_cuda or not out.is_contiguous():
+            raise ValueError(f'out must be a contiguous CUDA float64 tensor of shape {tuple(x.shape)}')
+        self.h.call(fn, kind, x.shape[1], _ptr(x), _ptr(out), _stream())
         return out
 
     # ---- state ---------------------------------------------------------------------------
@@ -111,19 +115,25 @@ class Window:
         B = au.shape[1]
         self.e.h.call('mpsw_window_ad', int(precision), B, _ptr(au), _ptr(ah), _stream())
 
-    def tl(self, du: torch.Tensor, dh: torch.Tensor, precision: int = FP64):
-        """Tangent linear of the window for B members (reference order in and out)."""
-        du_i = self.e.to_internal(du, _EDGE)
-        dh_i = self.e.to_internal(dh, _CELL)
-        self.tl_internal(du_i, dh_i, precision)
-        return self.e.to_reference(du_i, _EDGE), self.e.to_reference(dh_i, _CELL)
+    def tl(self, du: torch.Tensor, dh: torch.Tensor, precision: int = FP64, work=None, out=None):
+        """Tangent linear of the window for B members (reference order in and out).
 
-    def ad(self, au: torch.Tensor, ah: torch.Tensor, precision: int = FP64):
-        """Adjoint of the window for B members: final-state adjoints in, initial-state out."""
-        au_i = self.e.to_internal(au, _EDGE)
-        ah_i = self.e.to_internal(ah, _CELL)
-        self.ad_internal(au_i, ah_i, precision)
-        return self.e.to_reference(au_i, _EDGE), self.e.to_reference(ah_i, _CELL)
+        work: optional (u, h) internal-order scratch and out: optional (u, h) results, each
+        contiguous CUDA float64 of the members' shapes, so repeated sweeps allocate nothing."""
+        return self._sweep(self.tl_internal, du, dh, precision, work, out)
+
+    def ad(self, au: torch.Tensor, ah: torch.Tensor, precision: int = FP64, work=None, out=None):
+        """Adjoint of the window for B members: final-state adjoints in, initial-state out
+        (work, out as for tl)."""
+        return self._sweep(self.ad_internal, au, ah, precision, work, out)
+
+    def _sweep(self, fn, xu, xh, precision, work, out):
+        wu, wh = work if work is not None else (None, None)
+        ou, oh = out if out is not None else (None, None)
+        xu_i = self.e.to_internal(xu, _EDGE, wu)
+        xh_i = self.e.to_internal(xh, _CELL, wh)
+        fn(xu_i, xh_i, precision)
+        return self.e.to_reference(xu_i, _EDGE, ou), self.e.to_reference(xh_i, _CELL, oh)
 
 
 class RK4Step(torch.autograd.Function):
