@@ -33,9 +33,10 @@ UNITS = [
     ('mpsw_noalloc.cu', ['--fmad=false']),
     ('mpsw_ic.cu', ['--fmad=false']),
     ('mpsw_setup.cpp', ['--fmad=false', '-x', 'cu']),
+    ('mpsw_tiles.cpp', ['--fmad=false', '-x', 'cu']),
 ]
 HEADERS = ['mpsw_internal.h', 'mpsw_kernels.cuh', 'mpsw_launch.h', 'mpsw_launch.cuh', 'mpsw_members.cuh',
-           'mpsw_setup.h', 'mpsw_engine.h']
+           'mpsw_fused.cuh', 'mpsw_setup.h', 'mpsw_tiles.h', 'mpsw_engine.h']
 
 
 def _nvcc():

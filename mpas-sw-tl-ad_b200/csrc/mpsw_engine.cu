@@ -403,6 +403,47 @@ void Engine::free_device_mesh() {
   for (void *p : mesh_bufs) cudaFree(p);
   mesh_bufs.clear();
   mesh_built = false;
+  fused = FusedDev();
+  fused_K = 0;
+}
+
+// Halo tiles and coefficients of the fused FP32 member stages (meshes with at most 6 edges per
+// cell and 10 edgesOnEdge).  MPSW_FUSED=0 leaves them unbuilt (the sweeps then use the split
+// member kernels); MPSW_FUSED_K sets the owned cells per tile (default 64).
+void Engine::build_fused() {
+  fused = FusedDev();
+  fused_K = 0;
+  const char *on = getenv("MPSW_FUSED");
+  if (on && atoi(on) == 0) return;
+  if (m32.max_eoe > 10 || m32.max_eoc > 6) return;  // the tiles hold 10 edgesOnEdge, 6 edges per cell
+  const char *ke = getenv("MPSW_FUSED_K");
+  const int K = ke && atoi(ke) > 0 ? atoi(ke) : 64;
+  TileSetHost th[2];
+  for (int a = 0; a < 2; a++) {
+    const std::string err = build_tiles(bm, K, a == 1, &th[a]);
+    if (!err.empty()) throw EngineError(MPSW_ERR_MESH, "fused tiles: " + err);
+  }
+  FusedCoefHost fc;
+  build_fused_coefficients(bm, &fc);
+  auto &o = mesh_bufs;
+  FusedMesh &f = fused.fm;
+  f.v_cc = up<float>(fc.v_cc, o); f.v_kr = up<float>(fc.v_kr, o); f.v_kc = up<float>(fc.v_kc, o);
+  f.v_sr = up<float>(fc.v_sr, o); f.c_kr = up<float>(fc.c_kr, o); f.c_kec = up<float>(fc.c_kec, o);
+  f.c_sdv = up<float>(fc.c_sdv, o); f.c_src = up<float>(fc.c_src, o); f.c_hk = up<float>(fc.c_hk, o);
+  f.e_rdv = up<float>(fc.e_rdv, o); f.e_rdc = up<float>(fc.e_rdc, o);
+  for (int a = 0; a < 2; a++) {
+    TileSetDev &d = a ? fused.ad : fused.tl;
+    const TileSetHost &t = th[a];
+    d.ntiles = t.ntiles;
+    d.cnt = up<int>(t.cnt, o); d.off = up<int>(t.off, o);
+    d.ge = up<int>(t.ge, o); d.gc = up<int>(t.gc, o); d.gv = up<int>(t.gv, o);
+    d.erec = up<uint16_t>(t.erec, o); d.crec = up<uint16_t>(t.crec, o); d.vrec = up<uint16_t>(t.vrec, o);
+    d.smem[0] = t.smem[0];
+    d.smem[1] = t.smem[1];
+  }
+  cuda_check(Launch<float, double>::fused_prepare(fused), "fused stage shared-memory limit");
+  fused.ok = true;
+  fused_K = K;
 }
 
 RefMesh Engine::ref_mesh() {
@@ -470,6 +511,7 @@ void Engine::build_device_mesh() {
   d_perm[1] = up<int>(bm.perm_e, mesh_bufs);
   d_perm[2] = up<int>(bm.perm_v, mesh_bufs);
   cuda_check(cudaGetDevice(&mesh_device), "cudaGetDevice");
+  build_fused();
   noalloc_prepare_device();
   mesh_built = true;
   mesh_dirty = false;

@@ -15,6 +15,7 @@
 #include "mpsw_internal.h"
 #include "mpsw_launch.h"
 #include "mpsw_setup.h"
+#include "mpsw_tiles.h"
 
 namespace mpsw {
 
@@ -119,6 +120,9 @@ struct Engine {
   const int *d_perm[3] = {nullptr, nullptr, nullptr};
   const int *d_cnb = nullptr;  // [MAXE][nCells] the cell across each edge of a cell
   int mesh_device = -1;        // the CUDA device the mesh (and everything derived) lives on
+  FusedDev fused;              // halo tiles and coefficients of the fused member stages
+  int fused_K = 0;             // owned cells per tile of `fused` (0: not built)
+  void build_fused();
 
   // work
   std::vector<void *> work;

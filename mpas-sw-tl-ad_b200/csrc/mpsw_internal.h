@@ -158,6 +158,42 @@ struct AdOut {
   const R *pad_in_u[3], *pad_in_h[3];
 };
 
+// ---- fused member stages (mpsw_fused.cuh, tiles built by mpsw_tiles.cpp) ----------------
+// Prefix sizes of a tile's local spaces; the meaning of each layer for the tangent-linear and
+// the adjoint stage is given in mpsw_tiles.h.
+enum TileLayer { E_OWN, E_MID, E_ALL, C_OWN, C_KE, C_MID, C_ALL, V_ALL, kTileCounts };
+
+// Halo tiles on the device: per tile its counts and the first of its edge / cell / vertex
+// records; per record the entity's internal index and its neighbours as 16-bit local indices.
+struct TileSetDev {
+  int ntiles = 0;
+  const int *cnt = nullptr, *off = nullptr;
+  const int *ge = nullptr, *gc = nullptr, *gv = nullptr;
+  const uint16_t *erec = nullptr, *crec = nullptr, *vrec = nullptr;
+  size_t smem[2] = {0, 0};  // dynamic shared memory of a block for 4 and 8 members per block
+};
+
+// Per-entity coefficients of the fused kernels (FP32, internal order, slot-major, zero in the
+// padded slots of a list).
+struct FusedMesh {
+  const float *v_cc = nullptr;   // [3][V] sign * dcEdge / areaTriangle (v_es order)
+  const float *v_kr = nullptr;   // [3][V] kite / areaTriangle (v_c order)
+  const float *v_kc = nullptr;   // [3][V] kite / areaCell of that cell (v_c order)
+  const float *v_sr = nullptr;   // [3][V] sign / dvEdge (v_es order)
+  const float *c_kr = nullptr;   // [6][C] kite / areaCell (c_vs order)
+  const float *c_kec = nullptr;  // [6][C] 0.25 dcEdge dvEdge / areaCell (c_es order)
+  const float *c_sdv = nullptr;  // [6][C] sign * dvEdge / areaCell (c_es order)
+  const float *c_src = nullptr;  // [6][C] sign / dcEdge (c_es order)
+  const float *c_hk = nullptr;   // [6][C] 0.5 on the cell's edges (c_es order)
+  const float *e_rdv = nullptr, *e_rdc = nullptr;  // [E] 1 / dvEdge, 1 / dcEdge
+};
+
+struct FusedDev {
+  bool ok = false;  // tiles and coefficients built (meshes within 6 edgesOnCell, 10 edgesOnEdge)
+  FusedMesh fm;
+  TileSetDev tl, ad;
+};
+
 // Up to kConvMax double arrays rounded to float by one launch (see convert_list).
 constexpr int kConvMax = 10;
 // up to kConvMax FP64 arrays, each rounded to FP32 into dst[i] and/or copied into dst64[i]

@@ -10,11 +10,14 @@
 
 #include "mpsw_kernels.cuh"
 #include "mpsw_launch.h"
+#include "mpsw_fused.cuh"
 #include "mpsw_members.cuh"
 
 namespace mpsw {
 
 constexpr int kThreads = 128;
+constexpr int kFusedThreads = 256;             // threads of a fused-stage block
+constexpr size_t kFusedSmemMax = 227 * 1024;   // shared memory a block may use
 
 // Grid and block for `total` threads: 128-thread blocks (measured faster than 256 for the
 // latency-bound gathers here), halved (down to 64) while that leaves fewer than two blocks per
@@ -383,6 +386,66 @@ void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> 
   const int k = which < 0 || which > 3 ? 3 : which;
   const int vk = ad_width<R, A>(B, in, w, out, ad_prefer<R>(k));
   MPSW_VDISPATCH(vk, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(k, m, B, bs, ph, in, sd, w, out, s)));
+}
+template <typename R, typename A>
+bool Launch<R, A>::fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M) {
+  constexpr bool f32 = std::is_same<R, float>::value && std::is_same<A, double>::value;
+  if (!f32 || !f.ok || (M != 4 && M != 8) || B % M) return false;
+  if (ph.visc2 > R(0) || ph.visc4 > R(0) || ph.wind || ph.drag) return false;
+  const int i = M == 8 ? 1 : 0;
+  return f.tl.smem[i] <= kFusedSmemMax && f.ad.smem[i] <= kFusedSmemMax;
+}
+template <typename R, typename A>
+cudaError_t Launch<R, A>::fused_prepare(const FusedDev &f) {
+  if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {
+    cudaError_t err = cudaSuccess;
+    auto raise = [&](const void *k, size_t bytes) {
+      if (bytes > kFusedSmemMax) return;
+      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (err == cudaSuccess) err = e;
+    };
+    raise((const void *)k_tl_fused<4>, f.tl.smem[0]);
+    raise((const void *)k_tl_fused<8>, f.tl.smem[1]);
+    raise((const void *)k_ad_fused<4>, f.ad.smem[0]);
+    raise((const void *)k_ad_fused<8>, f.ad.smem[1]);
+    return err;
+  } else {
+    (void)f;
+    return cudaSuccess;
+  }
+}
+template <typename R, typename A>
+void Launch<R, A>::tl_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut,
+                            const R *ht, const Phys<R> &ph, const RK<R, A> &rku, const RK<R, A> &rkh,
+                            cudaStream_t s) {
+  if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {
+    if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused tangent-linear stage not available here");
+    g_launches++;
+    const float a = ph.apvm * ph.dt;
+    const LaunchCfg c{f.tl.ntiles * (B / M), kFusedThreads, f.tl.smem[M == 8]};
+    if (M == 8)
+      launch_k(k_tl_fused<8>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, (int)g_stable_base);
+    else
+      launch_k(k_tl_fused<4>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, (int)g_stable_base);
+  } else {
+    throw std::invalid_argument("fused stages run FP32 members only");
+  }
+}
+template <typename R, typename A>
+void Launch<R, A>::ad_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B, const Base<R> &bs,
+                            const Phys<R> &ph, const AdIn<R> &in, const AdOut<R, A> &out, cudaStream_t s) {
+  if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {
+    if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused adjoint stage not available here");
+    g_launches++;
+    const float a = ph.apvm * ph.dt;
+    const LaunchCfg c{f.ad.ntiles * (B / M), kFusedThreads, f.ad.smem[M == 8]};
+    if (M == 8)
+      launch_k(k_ad_fused<8>, c, s, f.ad, f.fm, m, B, bs, a, in, out, (int)g_stable_base);
+    else
+      launch_k(k_ad_fused<4>, c, s, f.ad, f.fm, m, B, bs, a, in, out, (int)g_stable_base);
+  } else {
+    throw std::invalid_argument("fused stages run FP32 members only");
+  }
 }
 template <typename R, typename A>
 void Launch<R, A>::ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,

@@ -79,6 +79,16 @@ struct Launch {
   // one kernel of ad_stage (0 edge, 1 cell, 2 vertex, 3 final), for timing
   static void ad_part(int which, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
                       const AdIn<R> &in, const AdWork<R> &w, const AdOut<R, A> &out, cudaStream_t s);
+  // Fused member stages (FP32 members only; mpsw_fused.cuh): one kernel for a whole
+  // tangent-linear or adjoint stage, M = 4 or 8 members per block.  The physics must be the
+  // default (no viscosity, drag or wind) and the seeds empty; fused_ok() tells.
+  static bool fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M);
+  static void tl_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B, const Base<R> &bs, const R *ut,
+                       const R *ht, const Phys<R> &ph, const RK<R, A> &rku, const RK<R, A> &rkh, cudaStream_t s);
+  static void ad_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B, const Base<R> &bs, const Phys<R> &ph,
+                       const AdIn<R> &in, const AdOut<R, A> &out, cudaStream_t s);
+  // raise the fused kernels' dynamic shared-memory limit to what the tiles need
+  static cudaError_t fused_prepare(const FusedDev &f);
   static void ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,
                        const R *seed_th, A wu, A wh, R *tu, R *th, cudaStream_t s);
   static void recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea, A *u_ad,

@@ -438,6 +438,21 @@ void Engine::window_ensure() {
   if (win.pending) window_forward();
 }
 
+// Members per block of the fused stage kernels for B members of precision R (0: the split
+// member kernels run instead: FP64 members, physics beyond the fused kernels, or MPSW_FUSED=0).
+// MPSW_FUSED_M=4|8 chooses the chunk; the default is 4 (the smaller shared-memory footprint).
+template <typename R>
+static int fused_members(const Engine &E, int B, const Phys<R> &ph) {
+  if constexpr (std::is_same<R, double>::value) {
+    return 0;
+  } else {
+    const char *env = getenv("MPSW_FUSED_M");
+    const int forced = env ? atoi(env) : 0;
+    const int M = forced == 4 || forced == 8 ? forced : 4;
+    return Launch<R, double>::fused_ok(E.fused, B, ph, M) ? M : 0;
+  }
+}
+
 // Member work of tangent-linear stage k about the linearisation point bs.
 //
 // Stage 1 reads the FP64 member state directly when R is double; otherwise its FP32 rounding in
@@ -482,6 +497,10 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
       rht.t_in[j] = mb->tk_h[j];
       rut.wt[j] = rht.wt[j] = w[j];
     }
+  }
+  if (const int M = fused_members<R>(E, B, ph)) {
+    Launch<R, double>::tl_fused(E.fused, M, m, B, bs, uti, hti, ph, rut, rht, st);
+    return;
   }
   Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, st);
   Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, st);
@@ -593,7 +612,10 @@ static void ad_member_step(Engine &E, int prec, int B, double *au, double *ah, M
       out.wu = wu4;
       out.wh = w[3];
     }
-    Launch<R, double>::ad_stage(m, B, base(k), ph, in, none, mb->w, out, E.stream);
+    if (const int M = fused_members<R>(E, B, ph))
+      Launch<R, double>::ad_fused(E.fused, M, m, B, base(k), ph, in, out, E.stream);
+    else
+      Launch<R, double>::ad_stage(m, B, base(k), ph, in, none, mb->w, out, E.stream);
   }
 }
 
@@ -778,16 +800,23 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters,
       case 1: LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream); break;
       case 2: LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream); break;
       case 3: LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream); break;
-      case 8:  // one whole tangent-linear stage
+      case 8:  // one whole tangent-linear stage, as the sweeps run it
+        if (const int M = fused_members<R>(E, B, ph)) {
+          LR::tl_fused(E.fused, M, m, B, bs, mb->pu[0], mb->ph[0], ph, rku, rkh, E.stream);
+          break;
+        }
         LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], mb->d, E.stream);
         LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream);
         LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream);
         if (ph.visc4 > R(0)) LR::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
         LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream);
         break;
-      case 9: {  // one whole adjoint stage
+      case 9: {  // one whole adjoint stage, as the sweeps run it
         const AdSeeds<R> none{};
-        LR::ad_stage(m, B, bs, ph, in, none, mb->w, out, E.stream);
+        if (const int M = fused_members<R>(E, B, ph))
+          LR::ad_fused(E.fused, M, m, B, bs, ph, in, out, E.stream);
+        else
+          LR::ad_stage(m, B, bs, ph, in, none, mb->w, out, E.stream);
         break;
       }
       default: LR::ad_part(which - 4, m, B, bs, ph, in, mb->w, out, E.stream); break;

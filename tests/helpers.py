@@ -38,13 +38,13 @@ def setup(m, level, case='tc5', seed=0, tl=False, ad=False, ntracers=1, **cfg):
         m.sw_test_case_1()
     elif case == 'tc6':
         m.sw_test_case_6()
-    else:  # seeded balanced flow with mountains (benchmark initial condition)
+    else:  # seeded balanced flow, with mountains ('seeded') or over a flat bottom ('balanced')
         scaled = ic.scale_mesh(msh)
         for k in ('xCell', 'yCell', 'zCell', 'xVertex', 'yVertex', 'zVertex', 'xEdge', 'yEdge',
                   'zEdge', 'dvEdge', 'dcEdge', 'areaCell', 'areaTriangle', 'kiteAreasOnVertex'):
             setattr(m, k.lower(), np.asarray(scaled[k]).T)
         st = ic.balanced_flow(scaled, seed)
-        b = ic.mountains(scaled, seed + 1000)
+        b = ic.mountains(scaled, seed + 1000) if case == 'seeded' else np.zeros(msh['nCells'])
         m.fvertex = st['fVertex']
         m.fedge = st['fEdge']
         m.h_s = b
