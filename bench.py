@@ -368,6 +368,30 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
     return kb[name]
 
 
+def fused_bytes(name, nC, nE, nV, B, s=4, a=8):
+    """Bytes a fused stage launch must move (a middle stage as the sweeps and mpsw_time_kernel run
+    it; default physics): every mesh coefficient, linearisation-point value and member value it
+    touches, once.  Members: the stage's inputs (s), and the RK bookkeeping, which reads the FP64
+    state (a) and writes the next provisional state and the stage's tendency (tangent linear) or
+    its contribution and the next tendency adjoint (adjoint) (2 s): (3 s + a) per member value.
+    Mesh, tangent linear: vertex 3+3 coefficients and f, cell 3 x 6 coefficients, edge 10 weights
+    and two reciprocals; adjoint: both weight lists, dvEdge, dcEdge, cell 3 x 6 coefficients and
+    areaCell, vertex 2 x 3 coefficients, areaTriangle and f.  Base: 6 edge and 2 vertex fields."""
+    E, C, V = nE, nC, nV
+    mesh = s * (7 * V + 18 * C + 12 * E) if name == 'tl_stage' else s * (22 * E + 19 * C + 8 * V)
+    base = s * (6 * E + 2 * V)
+    return mesh + base + B * (E + C) * (3 * s + a)
+
+
+def survey_stage_bytes(nC, nE, nV, sum_eoe, B, s=4, a=8):
+    """The per-stage bytes M + B S of the path's algorithmic model: mesh read once per stage and,
+    per member, x_k read and x_k+1 written at s, x0 read and the accumulator read and written at
+    a: S = (N + E)(2 s + 3 a)."""
+    E, N, V, S = nE, nC, nV, sum_eoe
+    mesh = 4 * (2 * E + 2 * E + S + E + 2 * E + N + 3 * V + 3 * V) + s * (S + 2 * E + 2 * N + 3 * V + 2 * V)
+    return mesh + B * (N + E) * (2 * s + 3 * a)
+
+
 def traffic_of(kernel, level, B):
     """DRAM bytes (read + write) of one launch of `kernel`, from the committed ncu summary of
     that kernel on this workload (profiles/k_<kernel>_l<level>_b<B>_fp32.md: the read and write
@@ -539,26 +563,39 @@ def run_mpsw(a, rank, world):
     hbm = hbm or 6650.0
     gradient_batch(FP32, B, du_i, dh_i)  # leaves the buffers of this configuration in place
     sum_eoe = int(unit['nEdgesOnEdge'].sum())
-    kt = {}
     import ctypes
-    for i, name in enumerate(KERNELS):
+    fm, fk = ctypes.c_int(), ctypes.c_int()
+    eng.h.check(L.mpsw_window_fused(eng.h.ptr, FP32, B, ctypes.byref(fm), ctypes.byref(fk)), 'window_fused')
+    fused = fm.value > 0
+    # the kernels the sweeps launch: the two fused stage kernels, or the eight split ones
+    timed_k = ['tl_stage', 'ad_stage'] if fused else KERNELS
+    kt = {}
+    for name in timed_k:
         out = ctypes.c_double()
-        eng.h.check(L.mpsw_time_kernel(eng.h.ptr, i, FP32, B, 20, ctypes.byref(out)), 'time_kernel')
+        eng.h.check(L.mpsw_time_kernel(eng.h.ptr, KERNELS.index(name), FP32, B, 20, ctypes.byref(out)), 'time_kernel')
         kt[name] = out.value
-    vb = (ctypes.c_int * 16)()
-    eng.h.check(L.mpsw_window_tuning(eng.h.ptr, FP32, B, vb), 'window_tuning')
-    tuning = {k: {'v': vb[2 * i], 'block': vb[2 * i + 1]} for i, k in enumerate(KERNELS[:8])}
-    # every member kernel launches once per stage: the dominant one is the slowest
-    top = max(KERNELS[:8], key=lambda k: kt[k])
-    bytes_ = kernel_bytes(top, nC, nE, nV, sum_eoe, B, 4)
+
+    def kbytes(k):
+        return fused_bytes(k, nC, nE, nV, B) if fused else kernel_bytes(k, nC, nE, nV, sum_eoe, B, 4)
+    cand = ['tl_stage', 'ad_stage'] if fused else KERNELS[:8]
+    top = max(cand, key=lambda k: kt[k])  # every candidate launches once per stage
+    bytes_ = kbytes(top)
     ach = bytes_ / (kt[top] / 1e3) / 1e9
-    stages = {k: {'ms': kt[k], 'algorithmic_bytes': kernel_bytes(k, nC, nE, nV, sum_eoe, B, 4),
-                  'achieved_gbs': kernel_bytes(k, nC, nE, nV, sum_eoe, B, 4) / (kt[k] / 1e3) / 1e9}
+    s8d = survey_stage_bytes(nC, nE, nV, sum_eoe, B)
+    stages = {k: {'ms': kt[k], 'algorithmic_bytes': kbytes(k), 'achieved_gbs': kbytes(k) / (kt[k] / 1e3) / 1e9,
+                  'frac': kbytes(k) / (kt[k] / 1e3) / 1e9 / hbm,
+                  'frac_of_M_plus_BS': s8d / (kt[k] / 1e3) / 1e9 / hbm}
               for k in ('tl_stage', 'ad_stage')}
-    roof = {'bound': 'hbm', 'kernel': top, 'achieved': ach, 'peak': hbm, 'unit': 'GB/s',
-            'frac': ach / hbm, 'peak_source': peak_kind, 'traffic': traffic_of(top, a.level, B),
-            'algorithmic_bytes': bytes_, 'ms_per_launch': kt[top],
-            'kernel_ms': {k: kt[k] for k in KERNELS[:8]}, 'stages': stages, 'tuning': tuning}
+    roof = {'bound': 'hbm', 'kernel': ('k_tl_fused' if top == 'tl_stage' else 'k_ad_fused') if fused else top,
+            'achieved': ach, 'peak': hbm, 'unit': 'GB/s', 'frac': ach / hbm, 'peak_source': peak_kind,
+            'traffic': traffic_of(('tl_fused' if top == 'tl_stage' else 'ad_fused') if fused else top, a.level, B),
+            'algorithmic_bytes': bytes_, 'ms_per_launch': kt[top], 'timing': 'each launch alone after a 256 MB L2 flush',
+            'stage_bytes_M_plus_BS': s8d, 'kernel_ms': kt, 'stages': stages,
+            'fused': {'members_per_block': fm.value, 'tile_cells': fk.value} if fused else None}
+    if not fused:
+        vb = (ctypes.c_int * 16)()
+        eng.h.check(L.mpsw_window_tuning(eng.h.ptr, FP32, B, vb), 'window_tuning')
+        roof['tuning'] = {k: {'v': vb[2 * i], 'block': vb[2 * i + 1]} for i, k in enumerate(KERNELS[:8])}
 
     # host baseline: serial oracle on one core, bounded sample
     cpu = None

@@ -128,6 +128,13 @@ int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes);
  * environment keeps fixed defaults; MPSW_TUNE_CACHE=<file> keeps the choices in a text file
  * keyed by device, mesh size, precision and B, and reuses them). */
 int mpsw_window_tuning(mpsw_handle *h, int precision, int B, int *v_block);
+/* Whether the window's sweeps of B members in `precision` run the fused member-stage kernels
+ * (one kernel per tangent-linear or adjoint RK stage over halo tiles of the mesh) and with what
+ * shape: *members_per_block 4 or 8 and *tile_cells the owned cells per tile, or both 0 when the
+ * split member kernels run (FP64 members, del2 / del4 viscosity, bottom drag or wind stress,
+ * meshes beyond 6 edges per cell or 10 edgesOnEdge, MPSW_FUSED=0 in the environment when the
+ * mesh was built).  No counterpart in the reference. */
+int mpsw_window_fused(mpsw_handle *h, int precision, int B, int *members_per_block, int *tile_cells);
 /* Tangent linear over the window, B members in place: du [nEdges][B], dh [nCells][B]. */
 int mpsw_window_tl(mpsw_handle *h, int precision, int B, double *du, double *dh, void *stream);
 /* Adjoint over the window, B members in place: on entry the adjoint of the final state, on

@@ -972,6 +972,17 @@ int mpsw_window_tuning(mpsw_handle *h, int precision, int B, int *v_block) {
     }
   });
 }
+int mpsw_window_fused(mpsw_handle *h, int precision, int B, int *members_per_block, int *tile_cells) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) {
+    if (!members_per_block || !tile_cells) throw mpsw::EngineError(MPSW_ERR_ARG, "null output");
+    if (precision != 0 && precision != 1) throw mpsw::EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
+    if (B < 1) throw mpsw::EngineError(MPSW_ERR_ARG, "B must be positive");
+    e.prepare();
+    *members_per_block =
+        precision == 1 ? mpsw::fused_members<float>(e, B, mpsw::phys_as<float>(e.phys())) : 0;
+    *tile_cells = *members_per_block ? e.fused_K : 0;
+  });
+}
 int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes) {
   return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_storage(mode, max_bytes); });
 }
