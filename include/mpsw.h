@@ -128,6 +128,18 @@ int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes);
  * environment keeps fixed defaults; MPSW_TUNE_CACHE=<file> keeps the choices in a text file
  * keyed by device, mesh size, precision and B, and reuses them). */
 int mpsw_window_tuning(mpsw_handle *h, int precision, int B, int *v_block);
+/* Checkpointing of the following mpsw_window_init calls, for windows whose stages are not
+ * stored.  snapshots 0 (default): two-level checkpointing, a checkpoint every ckpt_every steps
+ * and, in the adjoint sweep, one replay of each segment keeping its steps' states (one extra
+ * forward over the window, ckpt_every states held).  snapshots s > 0: binomial reversal as in
+ * Griewank's revolve: only the window's start state and s snapshot states are held, and the
+ * adjoint sweep recomputes states by the schedule of fewest forward steps for s slots (the
+ * sw_rk4_adj of each step then recomputes its four RK stages, as src/mpas_sw_module.f90:815-878
+ * does).  Results are identical in every mode.  No counterpart in the reference, whose driver
+ * keeps every step's state in a file (demo/run-adj.py:40-55). */
+int mpsw_window_snapshots(mpsw_handle *h, int snapshots);
+/* Nonlinear steps recomputed by the last adjoint sweep to re-form states (0 over stored stages). */
+int mpsw_window_forward_steps(mpsw_handle *h, long long *steps);
 /* Whether the window's sweeps of B members in `precision` run the fused member-stage kernels
  * (one kernel per tangent-linear or adjoint RK stage over halo tiles of the mesh) and with what
  * shape: *members_per_block 4 or 8 and *tile_cells the owned cells per tile, or both 0 when the

@@ -63,6 +63,15 @@ struct Window {
     size_t slot = 0;   // elements per stage slot
     size_t off[9] = {};
   } st[2];
+  // Binomial reversal (snapshots > 0): the window keeps only its start state and reverses the
+  // adjoint with `snaps` snapshot slots, recomputing states by the schedule of least forward
+  // steps (bin_cost / bin_split over steps x snapshots); 0: two-level checkpointing.
+  int snap_req = 0;          // snapshots of the next windows (mpsw_window_snapshots)
+  int snaps = 0;             // snapshots of the current window
+  std::vector<double *> sn_u, sn_h;
+  std::vector<long long> bin_cost;
+  std::vector<int> bin_split;
+  long long forward_steps = 0;  // trajectory steps recomputed by the last adjoint sweep
   int store_mode = -1;        // -1 automatic, else a mask of the precisions to store
   double store_budget = 0;    // bytes for automatic mode (0: 40% of free device memory)
   // member buffers per precision (0 FP64, 1 FP32), allocated for the largest B seen
@@ -216,6 +225,7 @@ struct Engine {
   void window_free_trajectory();
   void window_init(int nsteps, int every, cudaStream_t s);
   void window_storage(int mode, double max_bytes);
+  void window_snapshots(int snapshots);
   void window_store_alloc(int nsteps);
   void window_store_free(int prec);
   void window_capture_state(cudaStream_t s);

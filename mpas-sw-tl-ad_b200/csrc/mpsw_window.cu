@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cstdio>
 #include <string>
 #include <cstring>
@@ -259,6 +260,11 @@ void Engine::window_free_trajectory() {
   for (double *p : W.ck_h) cudaFree(p);
   W.ck_u.clear();
   W.ck_h.clear();
+  for (double *p : W.sn_u) cudaFree(p);
+  for (double *p : W.sn_h) cudaFree(p);
+  W.sn_u.clear();
+  W.sn_h.clear();
+  W.snaps = 0;
   for (void *p : {(void *)W.seg_u, (void *)W.seg_h, (void *)W.fin_u, (void *)W.fin_h, (void *)W.x_u,
                   (void *)W.x_h})
     if (p) cudaFree(p);
@@ -323,12 +329,51 @@ static void traj_step(Engine &E, bool in_place, int prec, Hook &&hook, int store
   }
 }
 
+// Snapshots of the following windows: 0 two-level checkpointing (default), s > 0 binomial
+// reversal with s snapshot slots.
+void Engine::window_snapshots(int snapshots) {
+  if (snapshots < 0 || snapshots > 4096) throw EngineError(MPSW_ERR_ARG, "snapshots must be 0..4096");
+  win.snap_req = snapshots;
+}
+
+// Least forward steps T(n, s) to reverse n steps from a held start state with s free snapshot
+// slots, and the first advance that attains it (Griewank's binomial checkpointing, by dynamic
+// programming over T(n, s) = min_m m + T(n - m, s - 1) + T(m, s), T(1, s) = 0, and with no slot
+// T(n, 0) = n (n - 1) / 2: every step recomputed from the start).
+static void binomial_tables(int N, int S, std::vector<long long> &T, std::vector<int> &split) {
+  if ((double)N * N * S > 4e9) throw EngineError(MPSW_ERR_UNSUPPORTED, "binomial schedule too large: use fewer steps or snapshots");
+  const size_t L = (size_t)N + 1;
+  T.assign(L * (S + 1), 0);
+  split.assign(L * (S + 1), 0);
+  for (int s = 0; s <= S; s++)
+    for (int n = 2; n <= N; n++) {
+      if (s == 0) {
+        T[n] = (long long)n * (n - 1) / 2;
+        split[n] = n - 1;
+        continue;
+      }
+      long long best = -1;
+      int bm = 1;
+      for (int m = 1; m < n; m++) {
+        const long long c = m + T[(size_t)(s - 1) * L + (n - m)] + T[(size_t)s * L + m];
+        if (best < 0 || c < best) {
+          best = c;
+          bm = m;
+        }
+      }
+      T[(size_t)s * L + n] = best;
+      split[(size_t)s * L + n] = bm;
+    }
+}
+
 void Engine::window_init(int nsteps, int every, cudaStream_t s) {
   if (nsteps < 1 || every < 1) throw EngineError(MPSW_ERR_ARG, "window needs nsteps >= 1 and ckpt_every >= 1");
   prepare();
   Window &W = win;
-  const int ev = std::min(every, nsteps), nck = (nsteps + ev - 1) / ev;
-  if (W.nsteps && W.every == ev && W.nckpt == nck && W.x_u) {
+  const int snaps = W.snap_req;
+  // binomial reversal keeps only the start state as a checkpoint
+  const int ev = snaps ? nsteps : std::min(every, nsteps), nck = (nsteps + ev - 1) / ev;
+  if (W.nsteps && W.every == ev && W.nckpt == nck && W.snaps == snaps && W.x_u) {
     W.nsteps = nsteps;  // same checkpoint layout: reuse every buffer
     window_store_alloc(nsteps);
     window_capture_state(s);
@@ -338,6 +383,8 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
   W.nsteps = nsteps;
   W.every = ev;
   W.nckpt = nck;
+  W.snaps = snaps;
+  if (snaps) binomial_tables(nsteps, snaps, W.bin_cost, W.bin_split);
   // zero-filled, so the autotuner's first timings (before the forward sweep has written the
   // stage buffers) read finite values
   auto D = [&](size_t n) {
@@ -356,8 +403,14 @@ void Engine::window_init(int nsteps, int every, cudaStream_t s) {
     W.ck_u.push_back(D(nE));
     W.ck_h.push_back(D(nC));
   }
-  W.seg_u = D((size_t)W.every * nE);
-  W.seg_h = D((size_t)W.every * nC);
+  if (!snaps) {
+    W.seg_u = D((size_t)W.every * nE);
+    W.seg_h = D((size_t)W.every * nC);
+  }
+  for (int i = 0; i < snaps; i++) {
+    W.sn_u.push_back(D(nE));
+    W.sn_h.push_back(D(nC));
+  }
   W.fin_u = D(nE);
   W.fin_h = D(nC);
   W.x_u = D(nE);
@@ -624,6 +677,7 @@ static void window_ad_impl(Engine &E, int prec, int B, double *user_u, double *u
   Window &W = E.win;
   MemberBufs<R> *mb = members<R>(E, prec, B, E.stream);
   double *au = W.ms[prec].x_u, *ah = W.ms[prec].x_h;
+  W.forward_steps = 0;
   members_copy(E, B, au, ah, user_u, user_h);
   const MeshDev<R> &m = mesh_for<R>(E);
   const Phys<double> ph64 = E.phys();
@@ -652,6 +706,51 @@ static void window_ad_impl(Engine &E, int prec, int B, double *user_u, double *u
     return;
   }
   tinit();
+  auto copy_state = [&](double *du_, double *dh_, const double *su_, const double *sh_) {
+    cuda_check(cudaMemcpyAsync(du_, su_, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
+    cuda_check(cudaMemcpyAsync(dh_, sh_, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
+  };
+  auto advance = [&](int k) {  // k nonlinear steps of the state in x_u, x_h
+    for (int i = 0; i < k; i++) E.run_graph(E.graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(E, true, 0, [](int) {}); });
+    W.forward_steps += k;
+  };
+  auto adjoint_step = [&]() {  // the adjoint of the step that starts at x_u, x_h
+    E.run_graph(E.graph_key(3, prec, B, au, ah), [&]() {
+      traj_step(E, false, prec, [](int) {});
+      ad_member_step<R>(E, prec, B, au, ah, mb, ph, w, c, [&](int k) { return base_for<R>(W, k); });
+    });
+  };
+  if (W.snaps) {
+    // binomial reversal: steps [a, a + n) from the start state (su, sh) with s free slots; the
+    // slot a level writes is slot s - 1, below every slot an enclosing level still holds
+    const size_t L = (size_t)W.nsteps + 1;
+    std::function<void(int, int, int, const double *, const double *)> rev = [&](int a, int n, int s,
+                                                                                 const double *su, const double *sh) {
+      if (n == 1) {
+        copy_state(W.x_u, W.x_h, su, sh);
+        adjoint_step();
+        return;
+      }
+      if (s == 0) {  // no slot: recompute each step from the start, last step first
+        for (int i = n - 1; i >= 0; i--) {
+          copy_state(W.x_u, W.x_h, su, sh);
+          advance(i);
+          adjoint_step();
+        }
+        return;
+      }
+      const int m = W.bin_split[(size_t)s * L + n];
+      copy_state(W.x_u, W.x_h, su, sh);
+      advance(m);
+      copy_state(W.sn_u[s - 1], W.sn_h[s - 1], W.x_u, W.x_h);
+      rev(a + m, n - m, s - 1, W.sn_u[s - 1], W.sn_h[s - 1]);
+      rev(a, m, s, su, sh);
+    };
+    rev(0, W.nsteps, W.snaps, W.ck_u[0], W.ck_h[0]);
+    members_copy(E, B, user_u, user_h, au, ah);
+    cuda_check(cudaGetLastError(), "window_ad");
+    return;
+  }
   for (int s = W.nckpt - 1; s >= 0; s--) {
     const int first = s * W.every, len = std::min(W.every, W.nsteps - first);
     // replay the segment, keeping the start state of every step
@@ -660,16 +759,11 @@ static void window_ad_impl(Engine &E, int prec, int B, double *user_u, double *u
     for (int j = 0; j < len; j++) {
       cuda_check(cudaMemcpyAsync(W.seg_u + (size_t)j * E.nE, W.x_u, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "seg");
       cuda_check(cudaMemcpyAsync(W.seg_h + (size_t)j * E.nC, W.x_h, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "seg");
-      if (j + 1 < len) E.run_graph(E.graph_key(1, 0, 1, nullptr, nullptr), [&]() { traj_step(E, true, 0, [](int) {}); });
+      if (j + 1 < len) advance(1);
     }
     for (int j = len - 1; j >= 0; j--) {
-      cuda_check(cudaMemcpyAsync(W.x_u, W.seg_u + (size_t)j * E.nE, sizeof(double) * E.nE, cudaMemcpyDeviceToDevice, E.stream), "copy");
-      cuda_check(cudaMemcpyAsync(W.x_h, W.seg_h + (size_t)j * E.nC, sizeof(double) * E.nC, cudaMemcpyDeviceToDevice, E.stream), "copy");
-      E.run_graph(E.graph_key(3, prec, B, au, ah), [&]() {
-        // forward sweep of this step, keeping the four stages' linearisation points
-        traj_step(E, false, prec, [](int) {});
-        ad_member_step<R>(E, prec, B, au, ah, mb, ph, w, c, [&](int k) { return base_for<R>(W, k); });
-      });
+      copy_state(W.x_u, W.x_h, W.seg_u + (size_t)j * E.nE, W.seg_h + (size_t)j * E.nC);
+      adjoint_step();  // recomputes this step's four stages, then their adjoints
     }
   }
   members_copy(E, B, user_u, user_h, au, ah);
@@ -981,6 +1075,15 @@ int mpsw_window_fused(mpsw_handle *h, int precision, int B, int *members_per_blo
     *members_per_block =
         precision == 1 ? mpsw::fused_members<float>(e, B, mpsw::phys_as<float>(e.phys())) : 0;
     *tile_cells = *members_per_block ? e.fused_K : 0;
+  });
+}
+int mpsw_window_snapshots(mpsw_handle *h, int snapshots) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) { e.window_snapshots(snapshots); });
+}
+int mpsw_window_forward_steps(mpsw_handle *h, long long *steps) {
+  return mpsw::guarded(h, [&](mpsw::Engine &e) {
+    if (!steps) throw mpsw::EngineError(MPSW_ERR_ARG, "null output");
+    *steps = e.win.forward_steps;
   });
 }
 int mpsw_window_storage(mpsw_handle *h, int mode, double max_bytes) {

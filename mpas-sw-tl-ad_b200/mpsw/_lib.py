@@ -50,6 +50,8 @@ SIGNATURES = {
     'mpsw_window_init': (_c_int, [_vp, _c_int, _c_int, _vp]),
     'mpsw_window_storage': (_c_int, [_vp, _c_int, ctypes.c_double]),
     'mpsw_window_tuning': (_c_int, [_vp, _c_int, _c_int, ctypes.POINTER(_c_int)]),
+    'mpsw_window_snapshots': (_c_int, [_vp, _c_int]),
+    'mpsw_window_forward_steps': (_c_int, [_vp, ctypes.POINTER(_ll)]),
     'mpsw_window_fused': (_c_int, [_vp, _c_int, _c_int, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
     'mpsw_window_tl': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),
     'mpsw_window_ad': (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp]),

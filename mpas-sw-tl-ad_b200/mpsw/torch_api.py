@@ -80,8 +80,8 @@ class Engine:
 
     # ---- windows -------------------------------------------------------------------------
     def window(self, nsteps: int, ckpt_every: int = 16, storage: int = -1,
-               max_bytes: float = 0.0) -> 'Window':
-        return Window(self, nsteps, ckpt_every, storage, max_bytes)
+               max_bytes: float = 0.0, snapshots: int = 0) -> 'Window':
+        return Window(self, nsteps, ckpt_every, storage, max_bytes, snapshots)
 
 
 class Window:
@@ -90,15 +90,26 @@ class Window:
 
     ``storage`` selects whether every RK stage's linearisation point is also kept in device
     memory (``mpsw_window_storage``): -1 automatic (within ``max_bytes``, 0 = 40% of free
-    memory), 0 checkpoints only, 1 FP64, 2 FP32, 3 both.  Results do not depend on it."""
+    memory), 0 checkpoints only, 1 FP64, 2 FP32, 3 both.  ``snapshots`` > 0 reverses a window
+    whose stages are not stored by binomial checkpointing with that many snapshot states
+    (``mpsw_window_snapshots``) instead of checkpoints every ``ckpt_every`` steps.  Results do
+    not depend on either."""
 
     def __init__(self, engine: Engine, nsteps: int, ckpt_every: int = 16, storage: int = -1,
-                 max_bytes: float = 0.0):
+                 max_bytes: float = 0.0, snapshots: int = 0):
         self.e = engine
         self.nsteps = nsteps
         engine.module.sync()  # pending host-side edits of the module's state first
         engine.h.call('mpsw_window_storage', int(storage), float(max_bytes))
+        engine.h.call('mpsw_window_snapshots', int(snapshots))
         engine.h.call('mpsw_window_init', int(nsteps), int(ckpt_every), _stream())
+
+    def forward_steps(self) -> int:
+        """Nonlinear steps the last adjoint sweep recomputed to re-form states."""
+        import ctypes
+        n = ctypes.c_longlong()
+        self.e.h.call('mpsw_window_forward_steps', ctypes.byref(n))
+        return n.value
 
     def final_state(self):
         u = torch.empty(self.e.nE, 1, dtype=torch.float64, device='cuda')
