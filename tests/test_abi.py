@@ -71,3 +71,48 @@ def test_variable_table_matches_reference_module():
               'tend_u_ad', 'kiteAreasOnVertex', 'deriv_two', 'boundaryEdge'):
         assert n in names, n
     assert L.mpsw_var_name(-1) is None
+
+
+def _load_small_mesh(h, level=2):
+    """A valid level-2 mesh loaded through the C ABI (host only)."""
+    from helpers import mesh
+    m = mesh(level)
+    L = h.lib
+    for k, n in (('ncells', m['nCells']), ('nedges', m['nEdges']), ('nvertices', m['nVertices']),
+                 ('maxedges', m['maxEdges']), ('maxedges2', m['maxEdges2']), ('vertexdegree', 3), ('ntracers', 1)):
+        h.check(L.mpsw_set_scalar(h.ptr, k.encode(), n), k)
+    h.check(L.mpsw_var_allocation(h.ptr), 'alloc')
+    arrays = {}
+    for name in ('cellsOnEdge', 'verticesOnEdge', 'edgesOnEdge', 'nEdgesOnEdge', 'edgesOnCell', 'nEdgesOnCell',
+                 'cellsOnVertex', 'edgesOnVertex', 'cellsOnCell', 'verticesOnCell', 'weightsOnEdge', 'dcEdge',
+                 'dvEdge', 'areaCell', 'areaTriangle', 'kiteAreasOnVertex', 'xCell', 'yCell', 'zCell', 'xEdge',
+                 'yEdge', 'zEdge', 'xVertex', 'yVertex', 'zVertex', 'latCell', 'lonCell', 'latEdge', 'lonEdge',
+                 'latVertex', 'lonVertex', 'angleEdge', 'meshDensity'):
+        a = np.ascontiguousarray(m[name], dtype=np.int32 if name[0] in 'cvne' and 'On' in name else np.float64)
+        arrays[name] = a
+        h.check(L.mpsw_set_var(h.ptr, name.encode(), a.ctypes.data_as(ctypes.c_void_p), a.size), name)
+    return m, arrays
+
+
+def test_corrupt_mesh_is_refused_with_mesh_status():
+    """sw_mpas_init_block validates the mesh on the host before anything reaches a device: an
+    out-of-range index or an inconsistent count returns MPSW_ERR_MESH (3) with a message naming
+    the problem, instead of the reference's unchecked reads."""
+    MPSW_ERR_MESH = 3
+    h = _lib.Handle()
+    _load_small_mesh(h)
+    rc = h.lib.mpsw_sw_mpas_init_block(h.ptr)  # the intact mesh passes validation (then needs a GPU)
+    assert rc != MPSW_ERR_MESH, h.lib.mpsw_last_error(h.ptr)
+    h.close()
+    for name, corrupt in (('cellsOnEdge', lambda a, m: a.__setitem__((5, 0), m['nCells'] + 7)),
+                          ('edgesOnEdge', lambda a, m: a.__setitem__((3, 2), 0)),
+                          ('nEdgesOnCell', lambda a, m: a.__setitem__(4, 9))):
+        h = _lib.Handle()
+        m, arrays = _load_small_mesh(h)
+        a = arrays[name].copy()
+        corrupt(a, m)
+        h.check(h.lib.mpsw_set_var(h.ptr, name.encode(), a.ctypes.data_as(ctypes.c_void_p), a.size), name)
+        rc = h.lib.mpsw_sw_mpas_init_block(h.ptr)
+        assert rc == MPSW_ERR_MESH, (name, rc, h.lib.mpsw_last_error(h.ptr))
+        assert h.lib.mpsw_last_error(h.ptr)
+        h.close()
