@@ -30,7 +30,10 @@ enum {
   MPSW_ERR_STATE = 2,    /* call out of order (not allocated, mesh not initialised) */
   MPSW_ERR_MESH = 3,     /* mesh failed validation */
   MPSW_ERR_CUDA = 4,     /* CUDA runtime error */
-  MPSW_ERR_UNSUPPORTED = 5
+  MPSW_ERR_UNSUPPORTED = 5,
+  MPSW_ERR_NONFINITE = 6 /* a routine formed a NaN or infinite tendency (or tendency adjoint): its
+                            input state or members are corrupt, or the time step is unstable.
+                            The reference has no such check; its Fortran carries the NaNs on. */
 };
 
 /* ---- lifecycle ------------------------------------------------------------------------ */

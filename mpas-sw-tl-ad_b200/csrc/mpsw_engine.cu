@@ -197,6 +197,8 @@ void Engine::need_device() {
   cuda_check(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate");
   for (cudaEvent_t *ev : {&ev_fork, &ev_step, &ev_join})
     cuda_check(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaMalloc(&d_bad, sizeof(int)), "cudaMalloc flag");
+  cuda_check(cudaMemsetAsync(d_bad, 0, sizeof(int), stream), "clear flag");
 }
 
 Engine::~Engine() {
@@ -208,6 +210,7 @@ Engine::~Engine() {
   if (trc) cudaFree(trc);
   window_free();
   if (l2_flush) cudaFree(l2_flush);
+  if (d_bad) cudaFree(d_bad);
   for (cudaEvent_t ev : {ev_fork, ev_step, ev_join})
     if (ev) cudaEventDestroy(ev);
   if (side) cudaStreamDestroy(side);
@@ -612,7 +615,27 @@ void Engine::mark_recon(int g) {
   for (int i = 0; i < 5; i++) mark_written(var((std::string(kDiagNames[i]) + sfx).c_str()), g != 2);
 }
 
-Phys<double> Engine::phys() const { return phys_cache; }
+Phys<double> Engine::phys() const {
+  Phys<double> p = phys_cache;
+  p.bad = d_bad;
+  return p;
+}
+
+// The flag the tendency kernels raise on a non-finite value: cleared at the start of a routine
+// (prepare, or a window sweep), read when it has finished.
+void Engine::nonfinite_clear() {
+  if (d_bad) cuda_check(cudaMemsetAsync(d_bad, 0, sizeof(int), stream), "clear non-finite flag");
+}
+void Engine::nonfinite_check(const char *what) {
+  if (!d_bad) return;
+  int v = 0;
+  cuda_check(cudaMemcpyAsync(&v, d_bad, sizeof(int), cudaMemcpyDeviceToHost, stream), "read non-finite flag");
+  cuda_check(cudaStreamSynchronize(stream), what);
+  if (v)
+    throw EngineError(MPSW_ERR_NONFINITE, std::string(what) +
+                                              ": a tendency became non-finite (NaN or Inf); the state or the "
+                                              "members are corrupt or the time step is unstable");
+}
 
 void Engine::refresh_phys() {
   Phys<double> &p = phys_cache;
@@ -665,6 +688,7 @@ void Engine::tl_diag_run(const Base<double> &bs, const double *ut, const double 
 void Engine::check_launch(const char *what) {
   cuda_check(cudaGetLastError(), what);
   cuda_check(cudaStreamSynchronize(stream), what);
+  nonfinite_check(what);
 }
 
 // Lazily computed diagnostics of the state left by the last routine (the reference's final
@@ -718,6 +742,7 @@ void Engine::init_block() {  // src/mpas_sw_module.f90:495-526
 void Engine::prepare() {
   ensure_mesh();
   sync_inputs();
+  nonfinite_clear();
 }
 
 // rk weights (src/mpas_sw_module.f90:567-575)
@@ -856,7 +881,7 @@ void Engine::forward(int prec, int nsteps) {
   const Phys<double> ph64 = phys();
   Phys<float> ph{};
   ph.dt = (float)ph64.dt; ph.apvm = (float)ph64.apvm; ph.visc2 = (float)ph64.visc2; ph.visc4 = (float)ph64.visc4;
-  ph.wind = ph64.wind; ph.drag = ph64.drag; ph.tc1 = ph64.tc1; ph.sphere = ph64.sphere;
+  ph.wind = ph64.wind; ph.drag = ph64.drag; ph.tc1 = ph64.tc1; ph.sphere = ph64.sphere; ph.bad = ph64.bad;
   double w[4], c[4];
   rk_coeffs(ph64.dt, w, c);
   double *u0 = dv("u"), *h0 = dv("h");

@@ -199,6 +199,9 @@ struct Engine {
   void tl_diag_run(const Base<double> &bs, const double *ut, const double *ht, const Diag<double> &d,
                    const Phys<double> &ph);
   void check_launch(const char *what);
+  int *d_bad = nullptr;  // non-finite flag of the tendency kernels (Phys::bad)
+  void nonfinite_clear();
+  void nonfinite_check(const char *what);
   void materialize_pending();
   void finish_levels(std::initializer_list<const char *> names);
   AdSeeds<double> seeds(bool *any);

@@ -112,7 +112,7 @@ template <int M>
 __global__ void __launch_bounds__(256, 3) k_tl_fused(TileSetDev ts, FusedMesh fm, MeshDev<float> m, int B,
                                                      Base<float> bs, const float *__restrict__ ut,
                                                      const float *__restrict__ ht, float a, RK<float, double> rku,
-                                                     RK<float, double> rkh, int early) {
+                                                     RK<float, double> rkh, int *bad, int early) {
   constexpr int T = M / 4;
   const TileView tv = tile_view(ts, B, M);
   const int nEo = tv.n[E_OWN], nEm = tv.n[E_MID], nEa = tv.n[E_ALL], nCo = tv.n[C_OWN], nCk = tv.n[C_KE],
@@ -236,7 +236,10 @@ __global__ void __launch_bounds__(256, 3) k_tl_fused(TileSetDev ts, FusedMesh fm
     }
     const F4 qt = (0.5f * __ldg(bs.pe + g)) * f1 + 0.5f * f2 + (0.5f * sb) * sPE[x];
     const F4 grad = (ROW(sKE, r.c2) - ROW(sKE, r.c1)) + float(GRAVITY) * (ROW(sH, r.c2) - ROW(sH, r.c1));
-    rk_members<float, double, 4>(rku, (size_t)g * B + tv.b0 + 4 * s, qt - grad * __ldg(fm.e_rdc + g));
+    const F4 tut = qt - grad * __ldg(fm.e_rdc + g);
+#pragma unroll
+    for (int q = 0; q < 4; q++) flag_nonfinite(bad, tut.x[q]);
+    rk_members<float, double, 4>(rku, (size_t)g * B + tv.b0 + 4 * s, tut);
   }
 }
 
@@ -248,7 +251,7 @@ __global__ void __launch_bounds__(256, 3) k_tl_fused(TileSetDev ts, FusedMesh fm
 template <int M>
 __global__ void __launch_bounds__(256, 3) k_ad_fused(TileSetDev ts, FusedMesh fm, MeshDev<float> m, int B,
                                                      Base<float> bs, float a, AdIn<float> in,
-                                                     AdOut<float, double> out, int early) {
+                                                     AdOut<float, double> out, int *bad, int early) {
   constexpr int T = M / 4;
   const TileView tv = tile_view(ts, B, M);
   const int nEo = tv.n[E_OWN], nEm = tv.n[E_MID], nEa = tv.n[E_ALL], nCo = tv.n[C_OWN], nCk = tv.n[C_KE],
@@ -361,6 +364,8 @@ __global__ void __launch_bounds__(256, 3) k_ad_fused(TileSetDev ts, FusedMesh fm
     for (int j = 0; j < 10; j++) pu = pu + __ldg(m.e_wrev + (size_t)j * nE + g) * ROW(sVT, r.eoe[j]);
     const float dc = __ldg(m.e_dc + g), kc = ((0.5f * dc) * __ldg(m.e_dv + g)) * sUB[i];
     pu = pu + kc * (ROW(sKE, r.c1) + ROW(sKE, r.c2)) + dc * (ROW(sVO, r.v2) - ROW(sVO, r.v1));
+#pragma unroll
+    for (int q = 0; q < 4; q++) flag_nonfinite(bad, pu.x[q]);
     ad_emit<float, double, 4>(out, 1, (size_t)g * B + tv.b0 + 4 * s, pu, 1.f);
   }
   for (int x = tid; x < nCo * T; x += nt) {

@@ -70,6 +70,9 @@ template <typename R>
 struct Phys {
   R dt, apvm, visc2, visc4;
   int wind, drag, tc1, sphere;
+  // set to 1 by a tendency kernel that forms a non-finite (NaN / Inf) normal-velocity
+  // tendency or adjoint; null: not checked
+  int *bad = nullptr;
 };
 
 // Diagnostics of one state (B members, [n][B]); null pointers are not written.

@@ -32,6 +32,12 @@ __device__ __forceinline__ void pdl_begin() {
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)(total); \
        t += (long long)gridDim.x * blockDim.x)
 
+// Raise the non-finite flag (Phys::bad) when x is NaN or infinite.
+template <typename R>
+__device__ __forceinline__ void flag_nonfinite(int *bad, R x) {
+  if (bad && !isfinite(x)) *bad = 1;
+}
+
 template <typename R>
 __device__ __forceinline__ R ld(const R *p, size_t i) {
   return __ldg(p + i);
@@ -252,6 +258,7 @@ __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *
       const R kee = R(0.5) * (d.ke[c1] + d.ke[c2]);
       tu = tu - ((R(1.0e-3) * ld(u, e)) * sqrt(R(2) * kee)) / hee;
     }
+    if (ph.bad && !isfinite(tu)) *ph.bad = 1;
     if (tend_u) tend_u[e] = tu;
     if (rk.next) rk.next[e] = rk.frozen ? R(rk.x0[e]) : R(rk.x0[e] + rk.c * A(tu));
     if (rk.acc_out && !rk.frozen) rk.acc_out[e] = rk.acc_in[e] + rk.w * A(tu);

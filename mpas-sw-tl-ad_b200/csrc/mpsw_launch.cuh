@@ -424,9 +424,9 @@ void Launch<R, A>::tl_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
     const float a = ph.apvm * ph.dt;
     const LaunchCfg c{f.tl.ntiles * (B / M), kFusedThreads, f.tl.smem[M == 8]};
     if (M == 8)
-      launch_k(k_tl_fused<8>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, (int)g_stable_base);
+      launch_k(k_tl_fused<8>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
     else
-      launch_k(k_tl_fused<4>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, (int)g_stable_base);
+      launch_k(k_tl_fused<4>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
   } else {
     throw std::invalid_argument("fused stages run FP32 members only");
   }
@@ -440,9 +440,9 @@ void Launch<R, A>::ad_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
     const float a = ph.apvm * ph.dt;
     const LaunchCfg c{f.ad.ntiles * (B / M), kFusedThreads, f.ad.smem[M == 8]};
     if (M == 8)
-      launch_k(k_ad_fused<8>, c, s, f.ad, f.fm, m, B, bs, a, in, out, (int)g_stable_base);
+      launch_k(k_ad_fused<8>, c, s, f.ad, f.fm, m, B, bs, a, in, out, ph.bad, (int)g_stable_base);
     else
-      launch_k(k_ad_fused<4>, c, s, f.ad, f.fm, m, B, bs, a, in, out, (int)g_stable_base);
+      launch_k(k_ad_fused<4>, c, s, f.ad, f.fm, m, B, bs, a, in, out, ph.bad, (int)g_stable_base);
   } else {
     throw std::invalid_argument("fused stages run FP32 members only");
   }

@@ -666,6 +666,10 @@ __device__ __forceinline__ void tl_edge_tend_body(const MeshDev<R> &m, int B, co
           (((R(1.0e-3) * uu) * sq) * het) / (hh * hh);
   }
   const size_t o = (size_t)e * B + b;
+  if (ph.bad) {
+#pragma unroll
+    for (int i = 0; i < V; i++) flag_nonfinite(ph.bad, tut.x[i]);
+  }
   if (tend_u) stv<V>(tend_u + o, tut);
   rk_members<R, A, V>(rk, o, tut);
 }
@@ -1260,6 +1264,10 @@ __device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const 
   pu = pu + dv * ldv<V>(w.div_ad + (size_t)c1 * B + b);
   pu = pu + dc * ldv<V>(w.circ_ad + (size_t)v2 * B + b);
   pu = pu - dc * ldv<V>(w.circ_ad + (size_t)v1 * B + b);
+  if (ph.bad) {
+#pragma unroll
+    for (int i = 0; i < V; i++) flag_nonfinite(ph.bad, pu.x[i]);
+  }
   ad_emit<R, A, V>(out, 1, (size_t)e * B + b, pu, R(1));
 }
 

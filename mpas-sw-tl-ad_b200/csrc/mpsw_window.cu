@@ -154,7 +154,7 @@ template <typename R>
 Phys<R> phys_as(const Phys<double> &p) {
   Phys<R> q{};
   q.dt = R(p.dt); q.apvm = R(p.apvm); q.visc2 = R(p.visc2); q.visc4 = R(p.visc4);
-  q.wind = p.wind; q.drag = p.drag; q.tc1 = p.tc1; q.sphere = p.sphere;
+  q.wind = p.wind; q.drag = p.drag; q.tc1 = p.tc1; q.sphere = p.sphere; q.bad = p.bad;
   return q;
 }
 
@@ -790,9 +790,11 @@ void Engine::window_tl(int prec, int B, double *du, double *dh, cudaStream_t s) 
   if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
   if (prec != 0 && prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   join(s, stream, true);
+  nonfinite_clear();
   TuneScope scope(tuning(prec, B));
   if (prec == 0) window_tl_impl<double>(*this, prec, B, du, dh);
   else window_tl_impl<float>(*this, prec, B, du, dh);
+  nonfinite_check("window_tl");
   join(s, stream, false);
 }
 
@@ -803,9 +805,11 @@ void Engine::window_ad(int prec, int B, double *au, double *ah, cudaStream_t s) 
   if (prec != 0 && prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   join(s, stream, true);
   window_ensure();
+  nonfinite_clear();
   TuneScope scope(tuning(prec, B));
   if (prec == 0) window_ad_impl<double>(*this, prec, B, au, ah);
   else window_ad_impl<float>(*this, prec, B, au, ah);
+  nonfinite_check("window_ad");
   join(s, stream, false);
 }
 
