@@ -14,14 +14,14 @@ torch = pytest.importorskip('torch')
 
 def test_forward_step_reports_nonfinite_state():
     m = setup(MpasSwModule(), 3, 'seeded', dt=600.0)
-    u0 = m.u[0, 0].copy()
+    u0, h0 = m.u[0, 0].copy(), m.h[0, 0].copy()
     bad = u0.copy()
     bad[17] = np.nan
     m.u[0, 0] = bad
     with pytest.raises(RuntimeError, match=r'\(6\).*non-finite'):
         m.sw_rk4()
     m.u[0, 0] = u0
-    m.h[0, 0] = m.h[1, 0]
+    m.h[0, 0] = h0
     m.sw_rk4()  # a clean state steps again
     assert np.isfinite(m.u[0, 0]).all()
 
