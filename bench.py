@@ -38,11 +38,14 @@ def parse():
     p.add_argument('--steps', type=int, default=3)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='mpsw', choices=['mpsw', 'reference'])
-    p.add_argument('--workload', default='tlad', choices=['tlad', 'fwd', 'costs'],
+    p.add_argument('--workload', default='tlad', choices=['tlad', 'fwd', 'costs', 'long'],
                    help='tlad: batched TL+AD gradients (level 7, 288 steps of 75 s, B=64); '
                         'fwd: nonlinear forward with mountains (level 7, 1152 steps of 75 s), sim-days/s; '
-                        'costs: 64 cost-function gradients by one batched adjoint (level 6, 1152 steps of 150 s)')
-    p.add_argument('--batch', type=int, default=64)
+                        'costs: 64 cost-function gradients by one batched adjoint (level 6, 1152 steps of 150 s); '
+                        'long: TL+AD gradients over a day on level 8 (2160 steps of 40 s, B=16) with binomial '
+                        'checkpointing of 32 snapshots')
+    p.add_argument('--batch', type=int, default=None)
+    p.add_argument('--snapshots', type=int, default=None, help='binomial checkpointing snapshots (long: 32)')
     p.add_argument('--level', type=int, default=None)
     p.add_argument('--nsteps', type=int, default=None)
     p.add_argument('--dt', type=float, default=None)
@@ -56,7 +59,9 @@ def parse():
     p.add_argument('--profile', action='store_true',
                    help='only the timed batched windows (for profiler launch lists); no JSON line')
     a = p.parse_args()
-    dflt = {'tlad': (7, 288, 75.0), 'fwd': (7, 1152, 75.0), 'costs': (6, 1152, 150.0)}[a.workload]
+    dflt = {'tlad': (7, 288, 75.0), 'fwd': (7, 1152, 75.0), 'costs': (6, 1152, 150.0), 'long': (8, 2160, 40.0)}[a.workload]
+    a.batch = a.batch or (16 if a.workload == 'long' else 64)
+    a.snapshots = (32 if a.workload == 'long' else 0) if a.snapshots is None else a.snapshots
     a.level = dflt[0] if a.level is None else a.level
     a.nsteps = dflt[1] if a.nsteps is None else a.nsteps
     a.dt = dflt[2] if a.dt is None else a.dt
@@ -953,6 +958,88 @@ def spawn_ranks(n):
     return next((rc for rc in rcs if rc), 0)
 
 
+def run_long(a, rank, world):
+    """Long-window gradients (level 8 by default): the window's stages are not stored (they would
+    take hundreds of GB), so the tangent-linear sweep recomputes the trajectory alongside and the
+    adjoint sweep reverses it by binomial checkpointing with `snapshots` snapshot states,
+    recomputing each step's RK stages.  One bench step is one gradient batch (B members); the
+    FP64 window's dot-product test and the FP32 form's error against it are reported."""
+    import torch
+    from module_sw_mpas import MpasSwModule
+    from mpsw import _lib, replicas
+    from mpsw.torch_api import FP32, FP64, Engine, Window
+
+    dev = rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    unit, mesh, st = workload(a.level, a.dt)
+    from mpsw import ic
+    b = ic.mountains(mesh, 1000)
+    mod = MpasSwModule()
+    load_module(mod, unit, mesh, st, a.dt)
+    mod.h_s = b[None, :]
+    mod.h[0, 0] = st['h'] - b
+    mod.sw_mpas_init_block()
+    eng = Engine(mod)
+    L = _lib.load()
+    B = a.batch
+    nC, nE = unit['nCells'], unit['nEdges']
+    dh_h, du_h = perturbations(unit, B, seed=replicas.member_seed(4, rank))
+    du_i = eng.to_internal(torch.tensor(du_h, device='cuda'), 1)
+    dh_i = eng.to_internal(torch.tensor(dh_h, device='cuda'), 0)
+    stream = torch.cuda.current_stream()
+
+    def batch(prec, keep=False):
+        w = Window(eng, a.nsteps, a.ckpt, 0, 0.0, a.snapshots)
+        xu, xh = du_i.clone(), dh_i.clone()
+        w.tl_internal(xu, xh, prec)
+        tl = (xu.clone(), xh.clone()) if keep else None
+        w.ad_internal(xu, xh, prec)
+        return tl, (xu, xh), w.forward_steps()
+
+    batch(FP32)  # warm-up (graph capture)
+    times = []
+    launches0 = L.mpsw_launch_count()
+    with Clocks(dev) as clk:
+        for _ in range(a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _, _, fsteps = batch(FP32)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = (L.mpsw_launch_count() - launches0) / a.steps
+    ms = replicas.max_over_ranks(sum(times) / len(times), device='cuda')
+    value = world * B / (ms / 1e3)
+    tl32, ad32, _ = batch(FP32, keep=True)
+    tl64, ad64, _ = batch(FP64, keep=True)
+    # dot-product test of the FP64 window: <L dx, L dx> = <dx, L^T L dx> (the adjoint is seeded
+    # with the tangent-linear output)
+    lhs = (tl64[0] * tl64[0]).sum(0) + (tl64[1] * tl64[1]).sum(0)
+    rhs = (du_i * ad64[0]).sum(0) + (dh_i * ad64[1]).sum(0)
+    dot = float(((lhs - rhs).abs() / lhs.abs()).max())
+    num = torch.sqrt(((ad32[0] - ad64[0]) ** 2).sum(0) + ((ad32[1] - ad64[1]) ** 2).sum(0))
+    den = torch.sqrt((ad64[0] ** 2).sum(0) + (ad64[1] ** 2).sum(0))
+    rel_err = float((num / den).max())
+    if rank == 0:
+        line = {
+            'metric': 'TL+AD gradients/s, long window, binomial checkpointing (FP32 stencils, FP64 accumulation)',
+            'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': a.steps, 'warmup': 1, 'ms_per_step': ms,
+            'step_ms': [round(t, 1) for t in times], 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32 stencils + f64 accumulation',
+            'data': 'synthetic (seeded balanced flow over 8 seeded mountains, level-%d TRiSK mesh)' % a.level,
+            'config': {'workload': 'long TL+AD window: level-%d mesh (%d cells), %d RK4 steps of %g s, %d members, '
+                                   'binomial checkpointing with %d snapshots' % (a.level, nC, a.nsteps, a.dt, B, a.snapshots),
+                       'parallelism': 'replicas x%d' % world},
+            'recomputed_forward_steps_in_adjoint': fsteps,
+            'fp64_dot_product_rel': dot,
+            'rel_err_fp32_vs_fp64': rel_err,
+            'clocks': clk.summary(),
+            'gpu_launches': int(launches),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if 'WORLD_SIZE' not in os.environ and a.gpus > 1 and a.impl == 'mpsw':
@@ -972,6 +1059,8 @@ def main():
         run_forward(a, rank, world)
     elif a.workload == 'costs':
         run_costs(a, rank, world)
+    elif a.workload == 'long':
+        run_long(a, rank, world)
     else:
         run_mpsw(a, rank, world)
     if world > 1 and a.impl == 'mpsw':
