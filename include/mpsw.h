@@ -159,6 +159,13 @@ int mpsw_window_ad(mpsw_handle *h, int precision, int B, double *au, double *ah,
 int mpsw_window_final_state(mpsw_handle *h, double *u, double *hh, void *stream);
 
 /* ---- initial conditions ------------------------------------------------------------------
+ * Williamson test case tc = 1, 2, 5 or 6 on the module's variables, as the reference's
+ * sw_test_case_1/2/5/6 (src/mpas_sw_testcases.f90:1-398) set it up, with the per-entity
+ * formulas evaluated by GPU kernels in FP64: the unit-sphere mesh is scaled by the Earth radius,
+ * then u(1), h(1), and as the case has them fEdge, fVertex, h_s, tracers(1) and the shifted
+ * lonCell are written.  Results agree with the host set-up to the last bits of sin / cos / pow. */
+int mpsw_sw_test_case(mpsw_handle *h, int tc);
+/*
  * Box average of a regular latitude-longitude field onto points, as the reference's grid2mpas
  * (src/grid2mpas.f90:21-70) does for its ERA5 initialisation: for each point (lat[k], lon[k], in
  * the units of the axes) the nearest axis entries (first minimum of the distance) and the mean

@@ -32,6 +32,7 @@ UNITS = [
     ('mpsw_window.cu', ['--fmad=false']),
     ('mpsw_noalloc.cu', ['--fmad=false']),
     ('mpsw_ic.cu', ['--fmad=false']),
+    ('mpsw_testcases.cu', ['--fmad=false']),
     ('mpsw_setup.cpp', ['--fmad=false', '-x', 'cu']),
     ('mpsw_tiles.cpp', ['--fmad=false', '-x', 'cu']),
 ]

@@ -218,6 +218,7 @@ struct Engine {
   void compute_tend(int tl);
   void reconstruct(int tl);
   void adjoint_at_state();
+  void test_case(int tc);  // Williamson test case on the GPU (mpsw_testcases.cu)
 
   // batched window (mpsw_window.cu)
   void graphs_free();

@@ -333,6 +333,15 @@ class MpasSwModule:
     def sw_test_case_6(self):
         _tc.test_case_6(self)
 
+    def sw_test_case_device(self, tc):
+        """Williamson test case ``tc`` (1, 2, 5 or 6) set up by GPU kernels instead of on the host
+        (no counterpart in the reference, whose sw_test_case_* this mirrors): the same fields as
+        sw_test_case_<tc>, to the last bit or two of the device's sin / cos / pow."""
+        scaled = ('xcell', 'ycell', 'zcell', 'xvertex', 'yvertex', 'zvertex', 'xedge', 'yedge', 'zedge',
+                  'dvedge', 'dcedge', 'areacell', 'areatriangle', 'kiteareasonvertex')
+        out = scaled + ('u', 'h', 'fedge', 'fvertex', 'h_s', 'loncell', 'tracers')
+        self._run('mpsw_sw_test_case', int(tc), reads=('u', 'h', 'tracers'), eager=out)
+
     # ---- access to the engine for the device-resident API -----------------------------------
     @property
     def handle(self):

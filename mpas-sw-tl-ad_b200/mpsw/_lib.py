@@ -50,6 +50,7 @@ SIGNATURES = {
     'mpsw_window_init': (_c_int, [_vp, _c_int, _c_int, _vp]),
     'mpsw_window_storage': (_c_int, [_vp, _c_int, ctypes.c_double]),
     'mpsw_window_tuning': (_c_int, [_vp, _c_int, _c_int, ctypes.POINTER(_c_int)]),
+    'mpsw_sw_test_case': (_c_int, [_vp, _c_int]),
     'mpsw_window_snapshots': (_c_int, [_vp, _c_int]),
     'mpsw_window_forward_steps': (_c_int, [_vp, ctypes.POINTER(_ll)]),
     'mpsw_window_fused': (_c_int, [_vp, _c_int, _c_int, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
