@@ -940,10 +940,11 @@ def run_costs(a, rank, world):
         print(json.dumps(line), flush=True)
 
 
-def spawn_ranks(n):
+def spawn_ranks(n, script=None, argv=None):
     """`bench.py --gpus N` started without a launcher: start N rank processes of this script (one
     per GPU, as torchrun would: RANK, LOCAL_RANK, WORLD_SIZE, MASTER_ADDR/PORT set), pass rank 0's
-    output through, and return the first nonzero exit status (0 when all succeed)."""
+    output through, and return the first nonzero exit status (0 when all succeed).  script / argv
+    default to this file and its command line."""
     import socket
     with socket.socket() as sk:
         sk.bind(('127.0.0.1', 0))
@@ -952,8 +953,8 @@ def spawn_ranks(n):
     for r in range(n):
         env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
                    MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
-        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env=env,
-                                      stdout=None if r == 0 else subprocess.DEVNULL))
+        cmd = [sys.executable, script or os.path.abspath(__file__)] + (sys.argv[1:] if argv is None else argv)
+        procs.append(subprocess.Popen(cmd, env=env, stdout=None if r == 0 else subprocess.DEVNULL))
     rcs = [p.wait() for p in procs]
     return next((rc for rc in rcs if rc), 0)
 

@@ -81,3 +81,18 @@ def test_two_ranks_gloo(total):
         assert res[r][0] == expect
         assert res[r][1] == 11.0
     assert res[0][2] != res[1][2]
+
+
+def test_bench_spawns_one_process_per_rank(capfd):
+    """bench.py --gpus N without a launcher starts N rank processes with the launcher's
+    environment; here they run a gloo probe and the job maximum reaches rank 0."""
+    import json
+    import os
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    rc = bench.spawn_ranks(2, script=os.path.join(root, 'tests', 'rank_probe.py'), argv=[])
+    assert rc == 0
+    line = [x for x in capfd.readouterr().out.splitlines() if x.startswith('{')][-1]
+    assert json.loads(line) == {'world': 2, 'max': 2.0, 'local_rank': 0}
