@@ -495,8 +495,12 @@ def run_mpsw(a, rank, world):
         import ctypes
         gradient_batch(FP32, B, du_i, dh_i)
         torch.cuda.synchronize()
+        fm, fk = ctypes.c_int(), ctypes.c_int()
+        eng.h.check(L.mpsw_window_fused(eng.h.ptr, FP32, B, ctypes.byref(fm), ctypes.byref(fk)), 'window_fused')
+        # the kernels the sweeps launch: the two fused stages (8, 9) or the eight split kernels
+        which = [8, 9] if fm.value else list(range(len(KERNELS) - 2))
         torch.cuda.nvtx.range_push('mpsw_kernels')
-        for i in range(len(KERNELS) - 2):
+        for i in which:
             out = ctypes.c_double()
             eng.h.check(L.mpsw_time_kernel(eng.h.ptr, i, FP32, B, 1, ctypes.byref(out)), 'time_kernel')
         torch.cuda.nvtx.range_pop()
