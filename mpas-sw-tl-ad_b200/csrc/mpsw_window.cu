@@ -790,8 +790,8 @@ void Engine::window_tl(int prec, int B, double *du, double *dh, cudaStream_t s) 
   if (mesh_dirty) throw EngineError(MPSW_ERR_STATE, "mesh changed since mpsw_window_init");
   if (prec != 0 && prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   join(s, stream, true);
-  nonfinite_clear();
   TuneScope scope(tuning(prec, B));
+  nonfinite_clear();  // after the autotuner, whose timings run on arbitrary buffer contents
   if (prec == 0) window_tl_impl<double>(*this, prec, B, du, dh);
   else window_tl_impl<float>(*this, prec, B, du, dh);
   nonfinite_check("window_tl");
@@ -805,8 +805,8 @@ void Engine::window_ad(int prec, int B, double *au, double *ah, cudaStream_t s) 
   if (prec != 0 && prec != 1) throw EngineError(MPSW_ERR_ARG, "precision must be 0 or 1");
   join(s, stream, true);
   window_ensure();
-  nonfinite_clear();
   TuneScope scope(tuning(prec, B));
+  nonfinite_clear();  // after the autotuner, whose timings run on arbitrary buffer contents
   if (prec == 0) window_ad_impl<double>(*this, prec, B, au, ah);
   else window_ad_impl<float>(*this, prec, B, au, ah);
   nonfinite_check("window_ad");
