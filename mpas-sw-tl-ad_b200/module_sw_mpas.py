@@ -154,7 +154,15 @@ class MpasSwModule:
             k = k.lower()
             if k in d['_arr'] and k not in d['_stale']:
                 self._push(k)
-        d['_h'].call(routine, *args)
+        try:
+            d['_h'].call(routine, *args)
+        except RuntimeError:
+            # a routine that failed part-way may have written its outputs on the device: the
+            # host copies of them are no longer current, so the next read fetches them
+            for k in tuple(eager) + tuple(lazy):
+                if k.lower() in d['_arr']:
+                    d['_stale'].add(k.lower())
+            raise
         for k in eager:
             k = k.lower()
             if k in d['_arr']:

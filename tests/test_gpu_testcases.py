@@ -31,7 +31,10 @@ def test_device_test_case_matches_host(tc):
     for k in FIELDS + ('tracers',):
         a, b = np.asarray(getattr(dev, k)), np.asarray(getattr(host, k))
         scale = max(np.abs(b).max(), 1e-300)
-        assert np.abs(a - b).max() <= 4e-15 * scale, (tc, k, np.abs(a - b).max() / scale)
+        # u is a difference of stream-function values ~1e8 apart from zero: their last-bit
+        # differences become ~1e-14 of u
+        tol = 1e-13 if k == 'u' else 4e-15
+        assert np.abs(a - b).max() <= tol * scale, (tc, k, np.abs(a - b).max() / scale)
 
 
 def test_device_test_case_level8_timing():
