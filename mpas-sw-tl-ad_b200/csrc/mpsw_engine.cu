@@ -411,13 +411,14 @@ void Engine::free_device_mesh() {
 }
 
 // Halo tiles and coefficients of the fused FP32 member stages (meshes with at most 6 edges per
-// cell and 10 edgesOnEdge).  MPSW_FUSED=0 leaves them unbuilt (the sweeps then use the split
-// member kernels); MPSW_FUSED_K sets the owned cells per tile (default 64).
+// cell and 10 edgesOnEdge), built when MPSW_FUSED=1 is set as the mesh goes to the device (the
+// sweeps use the split member kernels otherwise); MPSW_FUSED_K sets the owned cells per tile
+// (default 64).
 void Engine::build_fused() {
   fused = FusedDev();
   fused_K = 0;
   const char *on = getenv("MPSW_FUSED");
-  if (on && atoi(on) == 0) return;
+  if (!on || atoi(on) != 1) return;
   if (m32.max_eoe > 10 || m32.max_eoc > 6) return;  // the tiles hold 10 edgesOnEdge, 6 edges per cell
   const char *ke = getenv("MPSW_FUSED_K");
   const int K = ke && atoi(ke) > 0 ? atoi(ke) : 64;
