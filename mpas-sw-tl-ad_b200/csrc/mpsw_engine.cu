@@ -410,38 +410,32 @@ void Engine::free_device_mesh() {
   fused_K = 0;
 }
 
-// Halo tiles and coefficients of the fused FP32 member stages (meshes with at most 6 edges per
-// cell and 10 edgesOnEdge), built when MPSW_FUSED=1 is set as the mesh goes to the device (the
-// sweeps use the split member kernels otherwise); MPSW_FUSED_K sets the owned cells per tile
-// (default 64).
+// Halo tiles of the fused FP32 member stages (meshes with at most 6 edges per cell and 10
+// edgesOnEdge), built when MPSW_FUSED=1 is set as the mesh goes to the device (the sweeps use
+// the split member kernels otherwise).  MPSW_FUSED_SMEM sets the shared memory of a tile's block
+// in KB (default 100, two blocks per SM), MPSW_FUSED_K the most cells a tile owns (default 1024).
 void Engine::build_fused() {
   fused = FusedDev();
   fused_K = 0;
   const char *on = getenv("MPSW_FUSED");
   if (!on || atoi(on) != 1) return;
   if (m32.max_eoe > 10 || m32.max_eoc > 6) return;  // the tiles hold 10 edgesOnEdge, 6 edges per cell
-  const char *ke = getenv("MPSW_FUSED_K");
-  const int K = ke && atoi(ke) > 0 ? atoi(ke) : 64;
+  const char *ke = getenv("MPSW_FUSED_K"), *kb = getenv("MPSW_FUSED_SMEM");
+  const int K = ke && atoi(ke) > 0 ? atoi(ke) : 1024;
+  const size_t budget = (size_t)(kb && atoi(kb) > 0 ? atoi(kb) : 100) << 10;
   TileSetHost th[2];
   for (int a = 0; a < 2; a++) {
-    const std::string err = build_tiles(bm, K, a == 1, &th[a]);
+    const std::string err = build_tiles(bm, budget, K, a == 1, &th[a]);
     if (!err.empty()) throw EngineError(MPSW_ERR_MESH, "fused tiles: " + err);
   }
-  FusedCoefHost fc;
-  build_fused_coefficients(bm, &fc);
   auto &o = mesh_bufs;
-  FusedMesh &f = fused.fm;
-  f.v_cc = up<float>(fc.v_cc, o); f.v_kr = up<float>(fc.v_kr, o); f.v_kc = up<float>(fc.v_kc, o);
-  f.v_sr = up<float>(fc.v_sr, o); f.c_kr = up<float>(fc.c_kr, o); f.c_kec = up<float>(fc.c_kec, o);
-  f.c_sdv = up<float>(fc.c_sdv, o); f.c_src = up<float>(fc.c_src, o); f.c_hk = up<float>(fc.c_hk, o);
-  f.e_rdv = up<float>(fc.e_rdv, o); f.e_rdc = up<float>(fc.e_rdc, o);
   for (int a = 0; a < 2; a++) {
     TileSetDev &d = a ? fused.ad : fused.tl;
     const TileSetHost &t = th[a];
     d.ntiles = t.ntiles;
-    d.cnt = up<int>(t.cnt, o); d.off = up<int>(t.off, o);
-    d.ge = up<int>(t.ge, o); d.gc = up<int>(t.gc, o); d.gv = up<int>(t.gv, o);
-    d.erec = up<uint16_t>(t.erec, o); d.crec = up<uint16_t>(t.crec, o); d.vrec = up<uint16_t>(t.vrec, o);
+    d.cnt = up<int>(t.cnt, o);
+    d.blob_off = up<long long>(t.blob_off, o);
+    d.blob = up<unsigned char>(t.blob, o);
     d.smem[0] = t.smem[0];
     d.smem[1] = t.smem[1];
   }

@@ -162,38 +162,70 @@ struct AdOut {
 };
 
 // ---- fused member stages (mpsw_fused.cuh, tiles built by mpsw_tiles.cpp) ----------------
+#ifdef __CUDACC__
+#define MPSW_HD __host__ __device__
+#else
+#define MPSW_HD
+#endif
+
 // Prefix sizes of a tile's local spaces; the meaning of each layer for the tangent-linear and
 // the adjoint stage is given in mpsw_tiles.h.
 enum TileLayer { E_OWN, E_MID, E_ALL, C_OWN, C_KE, C_MID, C_ALL, V_ALL, kTileCounts };
 
-// Halo tiles on the device: per tile its counts and the first of its edge / cell / vertex
-// records; per record the entity's internal index and its neighbours as 16-bit local indices.
+// Sections of a tile's blob: everything a fused stage needs of the mesh for that tile, in the
+// tile's local order, copied into shared memory once per tile.  Internal indices (ge, gc, gv),
+// neighbour records as 16-bit local indices (vertex 16 B, cell 48 B, edge 32 B), and per-entity
+// coefficient records of 8 / 16 / 12 / 24 floats (their content per stage: mpsw_tiles.cpp).
+enum BlobSection { B_GE, B_GC, B_GV, B_VREC, B_CREC, B_EREC, B_VCOEF, B_C1, B_C2, B_C3, B_ECOEF, kBlobSections };
+
+MPSW_HD inline int blob_up16(int x) { return (x + 15) & ~15; }
+
+// Byte offsets of the sections of a tile's blob from its counts; returns the blob's size.
+MPSW_HD inline int blob_layout(const int *cnt, bool adjoint, int *off) {
+  int sz[kBlobSections];
+  sz[B_GE] = 4 * cnt[E_ALL];
+  sz[B_GC] = 4 * cnt[C_ALL];
+  sz[B_GV] = 4 * cnt[V_ALL];
+  sz[B_VREC] = 16 * cnt[V_ALL];
+  sz[B_CREC] = 48 * cnt[C_MID];
+  sz[B_EREC] = 32 * cnt[E_MID];
+  sz[B_VCOEF] = 32 * cnt[V_ALL];
+  sz[B_C1] = 32 * cnt[C_MID];
+  sz[B_C2] = adjoint ? 64 * cnt[C_OWN] : 32 * cnt[C_KE];
+  sz[B_C3] = adjoint ? 0 : 32 * cnt[C_OWN];
+  sz[B_ECOEF] = (adjoint ? 96 : 48) * cnt[E_MID];
+  int o = 0;
+  for (int k = 0; k < kBlobSections; k++) {
+    off[k] = o;
+    o += blob_up16(sz[k]);
+  }
+  return o;
+}
+
+// Floats of the linearisation point a fused stage stages per tile (see mpsw_fused.cuh).
+MPSW_HD inline int base_floats(const int *cnt, bool adjoint) {
+  return blob_up16(4 * ((adjoint ? 3 : 2) * cnt[E_ALL] + (adjoint ? 3 : 4) * cnt[E_MID] + 2 * cnt[V_ALL])) / 4;
+}
+
+// Member rows (M floats each) of a fused stage's block: inputs double-buffered, then the
+// stage's intermediates (see mpsw_fused.cuh).
+MPSW_HD inline int member_rows(const int *cnt, bool adjoint) {
+  const int in = 2 * (cnt[E_ALL] + cnt[C_ALL]);
+  return adjoint ? in + 3 * cnt[E_MID] + cnt[E_OWN] + cnt[C_MID] + cnt[C_KE] + 2 * cnt[V_ALL]
+                 : in + cnt[V_ALL] + cnt[C_MID] + cnt[C_KE] + 2 * cnt[E_MID] + cnt[E_OWN];
+}
+
+// Halo tiles on the device: per tile its counts and the byte offset of its blob.
 struct TileSetDev {
   int ntiles = 0;
-  const int *cnt = nullptr, *off = nullptr;
-  const int *ge = nullptr, *gc = nullptr, *gv = nullptr;
-  const uint16_t *erec = nullptr, *crec = nullptr, *vrec = nullptr;
-  size_t smem[2] = {0, 0};  // dynamic shared memory of a block for 4 and 8 members per block
-};
-
-// Per-entity coefficients of the fused kernels (FP32, internal order, slot-major, zero in the
-// padded slots of a list).
-struct FusedMesh {
-  const float *v_cc = nullptr;   // [3][V] sign * dcEdge / areaTriangle (v_es order)
-  const float *v_kr = nullptr;   // [3][V] kite / areaTriangle (v_c order)
-  const float *v_kc = nullptr;   // [3][V] kite / areaCell of that cell (v_c order)
-  const float *v_sr = nullptr;   // [3][V] sign / dvEdge (v_es order)
-  const float *c_kr = nullptr;   // [6][C] kite / areaCell (c_vs order)
-  const float *c_kec = nullptr;  // [6][C] 0.25 dcEdge dvEdge / areaCell (c_es order)
-  const float *c_sdv = nullptr;  // [6][C] sign * dvEdge / areaCell (c_es order)
-  const float *c_src = nullptr;  // [6][C] sign / dcEdge (c_es order)
-  const float *c_hk = nullptr;   // [6][C] 0.5 on the cell's edges (c_es order)
-  const float *e_rdv = nullptr, *e_rdc = nullptr;  // [E] 1 / dvEdge, 1 / dcEdge
+  const int *cnt = nullptr;
+  const long long *blob_off = nullptr;
+  const unsigned char *blob = nullptr;
+  size_t smem[2] = {0, 0};  // dynamic shared memory of a block for 4 and 8 members per chunk
 };
 
 struct FusedDev {
-  bool ok = false;  // tiles and coefficients built (meshes within 6 edgesOnCell, 10 edgesOnEdge)
-  FusedMesh fm;
+  bool ok = false;  // tiles built (meshes within 6 edgesOnCell, 10 edgesOnEdge)
   TileSetDev tl, ad;
 };
 

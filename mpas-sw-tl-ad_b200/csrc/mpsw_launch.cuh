@@ -387,6 +387,15 @@ void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> 
   const int vk = ad_width<R, A>(B, in, w, out, ad_prefer<R>(k));
   MPSW_VDISPATCH(vk, MPSW_BDISPATCH(m, ad_launch<R, A, VV, NB>(k, m, B, bs, ph, in, sd, w, out, s)));
 }
+// Chunks of M members one fused-stage block walks (all B / M of its tile by default; fewer
+// blocks per tile take more chunks each, so the tile's blob is staged fewer times).
+// MPSW_FUSED_CPB overrides it when it divides B / M.
+inline int fused_cpb(int B, int M) {
+  const int chunks = B / M;
+  const char *e = std::getenv("MPSW_FUSED_CPB");
+  const int v = e ? std::atoi(e) : 0;
+  return v > 0 && chunks % v == 0 ? v : chunks;
+}
 template <typename R, typename A>
 bool Launch<R, A>::fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M) {
   constexpr bool f32 = std::is_same<R, float>::value && std::is_same<A, double>::value;
@@ -419,14 +428,16 @@ void Launch<R, A>::tl_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
                             const R *ht, const Phys<R> &ph, const RK<R, A> &rku, const RK<R, A> &rkh,
                             cudaStream_t s) {
   if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {
+    (void)m;
     if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused tangent-linear stage not available here");
     g_launches++;
     const float a = ph.apvm * ph.dt;
-    const LaunchCfg c{f.tl.ntiles * (B / M), kFusedThreads, f.tl.smem[M == 8]};
+    const int cpb = fused_cpb(B, M);
+    const LaunchCfg c{f.tl.ntiles * ((B / M) / cpb), kFusedThreads, f.tl.smem[M == 8]};
     if (M == 8)
-      launch_k(k_tl_fused<8>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
+      launch_k(k_tl_fused<8>, c, s, f.tl, B, cpb, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
     else
-      launch_k(k_tl_fused<4>, c, s, f.tl, f.fm, m, B, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
+      launch_k(k_tl_fused<4>, c, s, f.tl, B, cpb, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
   } else {
     throw std::invalid_argument("fused stages run FP32 members only");
   }
@@ -435,14 +446,16 @@ template <typename R, typename A>
 void Launch<R, A>::ad_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B, const Base<R> &bs,
                             const Phys<R> &ph, const AdIn<R> &in, const AdOut<R, A> &out, cudaStream_t s) {
   if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {
+    (void)m;
     if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused adjoint stage not available here");
     g_launches++;
     const float a = ph.apvm * ph.dt;
-    const LaunchCfg c{f.ad.ntiles * (B / M), kFusedThreads, f.ad.smem[M == 8]};
+    const int cpb = fused_cpb(B, M);
+    const LaunchCfg c{f.ad.ntiles * ((B / M) / cpb), kFusedThreads, f.ad.smem[M == 8]};
     if (M == 8)
-      launch_k(k_ad_fused<8>, c, s, f.ad, f.fm, m, B, bs, a, in, out, ph.bad, (int)g_stable_base);
+      launch_k(k_ad_fused<8>, c, s, f.ad, B, cpb, bs, a, in, out, ph.bad, (int)g_stable_base);
     else
-      launch_k(k_ad_fused<4>, c, s, f.ad, f.fm, m, B, bs, a, in, out, ph.bad, (int)g_stable_base);
+      launch_k(k_ad_fused<4>, c, s, f.ad, B, cpb, bs, a, in, out, ph.bad, (int)g_stable_base);
   } else {
     throw std::invalid_argument("fused stages run FP32 members only");
   }

@@ -40,21 +40,19 @@ struct TileSetHost {
   int K = 0, ntiles = 0;
   int max_cnt[kTileCounts] = {};            // largest count of each layer over the tiles
   std::vector<int> cnt;                     // [ntiles][kTileCounts]
-  std::vector<int> off;                     // [ntiles][3] first edge / cell / vertex record
-  std::vector<int> ge, gc, gv;              // internal index of each record
-  std::vector<uint16_t> erec, crec, vrec;   // records, strides kERec / kCRec / kVRec
+  std::vector<int> off;                     // [ntiles][3] first edge / cell / vertex of ge / gc / gv
+  std::vector<int> ge, gc, gv;              // internal index of each local entity, tile after tile
+  std::vector<unsigned char> blob;          // the tiles' blobs (BlobSection), each 16-byte aligned
+  std::vector<long long> blob_off;          // [ntiles] byte offset of each tile's blob
   size_t smem[2] = {0, 0};                  // shared memory of the stage's block, 4 / 8 members
 };
 
-// Build the tangent-linear (adjoint = false) or adjoint tiles of K owned cells for a mesh with
-// at most 6 edges per cell and 10 edgesOnEdge.  Returns an empty string or the problem found
-// (a local space above 65534 entities, or a phase that would read outside its tile).
-std::string build_tiles(const BuiltMesh &m, int K, bool adjoint, TileSetHost *out);
-
-// Coefficients of the fused kernels (FusedMesh in mpsw_internal.h), formed in FP64 and rounded.
-struct FusedCoefHost {
-  std::vector<float> v_cc, v_kr, v_kc, v_sr, c_kr, c_kec, c_sdv, c_src, c_hk, e_rdv, e_rdc;
-};
-void build_fused_coefficients(const BuiltMesh &m, FusedCoefHost *out);
+// Build the tangent-linear (adjoint = false) or adjoint tiles for a mesh with at most 6 edges
+// per cell and 10 edgesOnEdge, with their blobs (coefficients formed in FP64 from the mesh and
+// rounded to FP32).  Each tile owns a run of consecutive cells of the internal order, as long as
+// its block's shared memory with 4 members per chunk stays within `budget` bytes and at most
+// `kmax` cells.  Returns an empty string or the problem found (a cell whose halo alone exceeds
+// the budget, or a phase that would read outside its tile).
+std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, bool adjoint, TileSetHost *out);
 
 }  // namespace mpsw

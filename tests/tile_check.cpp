@@ -16,7 +16,7 @@ extern "C" int tile_check(int nC, int nE, int nV, int maxEdges, int maxEdges2, c
                           const int *eoe, const int *neoe, const int *eoc, const int *neoc, const int *cov,
                           const int *eov, const double *w, const double *kites, const double *dc,
                           const double *dv, const double *ac, const double *at, const double *xyz[9], int K,
-                          int adjoint, long long *out, char *err, int errlen) {
+                          int budget_kb, int adjoint, long long *out, char *err, int errlen) {
   RefMesh r;
   r.nC = nC; r.nE = nE; r.nV = nV; r.maxEdges = maxEdges; r.maxEdges2 = maxEdges2; r.vd = 3;
   r.cellsOnEdge = coe; r.verticesOnEdge = voe; r.edgesOnEdge = eoe; r.nEdgesOnEdge = neoe;
@@ -32,7 +32,7 @@ extern "C" int tile_check(int nC, int nE, int nV, int maxEdges, int maxEdges2, c
   BuiltMesh bm;
   std::string e = build_mesh(r, g, 1, &bm);
   TileSetHost t;
-  if (e.empty()) e = build_tiles(bm, K, adjoint != 0, &t);
+  if (e.empty()) e = build_tiles(bm, (size_t)budget_kb << 10, K, adjoint != 0, &t);
   if (!e.empty()) {
     std::strncpy(err, e.c_str(), errlen - 1);
     err[errlen - 1] = 0;
