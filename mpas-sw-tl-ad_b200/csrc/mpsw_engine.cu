@@ -683,7 +683,6 @@ void Engine::tl_diag_run(const Base<double> &bs, const double *ut, const double 
 void Engine::check_launch(const char *what) {
   cuda_check(cudaGetLastError(), what);
   cuda_check(cudaStreamSynchronize(stream), what);
-  nonfinite_check(what);
 }
 
 // Lazily computed diagnostics of the state left by the last routine (the reference's final
@@ -854,6 +853,7 @@ void Engine::rk4(int nsteps) {  // src/mpas_sw_module.f90:528-635
   mark_recon(0);
   mark_diag(0, true);
   pending_diag = 1;
+  nonfinite_check("sw_rk4");  // after the bookkeeping: the outputs are on the device either way
 }
 
 // nsteps RK4 steps of the level-1 state.  Precision 0 is sw_rk4 repeated (bit-identical);
@@ -914,6 +914,7 @@ void Engine::forward(int prec, int nsteps) {
   mark_recon(0);
   mark_diag(0, true);
   pending_diag = 1;
+  nonfinite_check("forward");
 }
 
 // u(2) = u(1) after a step (src/mpas_sw_module.f90:631-632, 774-777)
@@ -963,6 +964,7 @@ void Engine::rk4_tlm(int nsteps) {  // src/mpas_sw_module.f90:637-781
   mark_diag(0, true);
   mark_diag(1, true);
   pending_diag = 2;
+  nonfinite_check("sw_rk4_tlm");
 }
 
 AdSeeds<double> Engine::seeds(bool *any) {
@@ -1065,6 +1067,7 @@ void Engine::rk4_adj() {  // src/mpas_sw_module.f90:783-1002
   mark_recon(0);
   mark_diag(0, true);
   pending_diag = 1;
+  nonfinite_check("sw_rk4_adj");
 }
 
 void Engine::solve_diagnostics(int tl) {
@@ -1103,6 +1106,7 @@ void Engine::compute_tend(int tl) {
     mark_written(var("tend_u_tl"), true);
     mark_written(var("tend_h_tl"), true);
   }
+  nonfinite_check("compute_tend");
 }
 
 void Engine::reconstruct(int tl) {
