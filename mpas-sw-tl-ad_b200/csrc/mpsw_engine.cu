@@ -412,20 +412,27 @@ void Engine::free_device_mesh() {
 
 // Halo tiles of the fused FP32 member stages (meshes with at most 6 edges per cell and 10
 // edgesOnEdge), built when MPSW_FUSED=1 is set as the mesh goes to the device (the sweeps use
-// the split member kernels otherwise).  MPSW_FUSED_SMEM sets the shared memory of a tile's block
-// in KB (default 100, two blocks per SM), MPSW_FUSED_K the most cells a tile owns (default 1024).
+// the split member kernels otherwise).  MPSW_FUSED_M sets the members per chunk the tiles are
+// sized for (4, 8 or 16; default 8), MPSW_FUSED_NT the threads per block (256, 512 or 1024;
+// default 512), MPSW_FUSED_SMEM the shared memory of a tile's block in KB (default 110) and
+// MPSW_FUSED_K the most cells a tile owns (default 1024).
 void Engine::build_fused() {
   fused = FusedDev();
   fused_K = 0;
   const char *on = getenv("MPSW_FUSED");
   if (!on || atoi(on) != 1) return;
   if (m32.max_eoe > 10 || m32.max_eoc > 6) return;  // the tiles hold 10 edgesOnEdge, 6 edges per cell
-  const char *ke = getenv("MPSW_FUSED_K"), *kb = getenv("MPSW_FUSED_SMEM");
-  const int K = ke && atoi(ke) > 0 ? atoi(ke) : 1024;
-  const size_t budget = (size_t)(kb && atoi(kb) > 0 ? atoi(kb) : 100) << 10;
+  auto env = [](const char *n, int dflt) {
+    const char *e = getenv(n);
+    return e && atoi(e) > 0 ? atoi(e) : dflt;
+  };
+  const int K = env("MPSW_FUSED_K", 1024), M = env("MPSW_FUSED_M", 8), NT = env("MPSW_FUSED_NT", 512);
+  const size_t budget = (size_t)env("MPSW_FUSED_SMEM", 110) << 10;
+  if (M != 4 && M != 8 && M != 16) throw EngineError(MPSW_ERR_ARG, "MPSW_FUSED_M must be 4, 8 or 16");
+  if (NT != 256 && NT != 512 && NT != 1024) throw EngineError(MPSW_ERR_ARG, "MPSW_FUSED_NT must be 256, 512 or 1024");
   TileSetHost th[2];
   for (int a = 0; a < 2; a++) {
-    const std::string err = build_tiles(bm, budget, K, a == 1, &th[a]);
+    const std::string err = build_tiles(bm, budget, K, M, a == 1, &th[a]);
     if (!err.empty()) throw EngineError(MPSW_ERR_MESH, "fused tiles: " + err);
   }
   auto &o = mesh_bufs;
@@ -436,9 +443,10 @@ void Engine::build_fused() {
     d.cnt = up<int>(t.cnt, o);
     d.blob_off = up<long long>(t.blob_off, o);
     d.blob = up<unsigned char>(t.blob, o);
-    d.smem[0] = t.smem[0];
-    d.smem[1] = t.smem[1];
+    for (int i = 0; i < 3; i++) d.smem[i] = t.smem[i];
   }
+  fused.M = M;
+  fused.nt = NT;
   cuda_check(Launch<float, double>::fused_prepare(fused), "fused stage shared-memory limit");
   fused.ok = true;
   fused_K = K;

@@ -163,8 +163,8 @@ __device__ __forceinline__ void prefetch_rows(const TileSmem &t, const float *xe
 // (src/mpas_sw_dyncore_tlm.f90) at one linearisation point, and the RK bookkeeping.
 // A block takes chunks [group * cpb, (group + 1) * cpb) of its tile's B / M member chunks.
 // ----------------------------------------------------------------------------------------
-template <int M>
-__global__ void __launch_bounds__(256, 2) k_tl_fused(TileSetDev ts, int B, int cpb, Base<float> bs,
+template <int M, int NT>
+__global__ void __launch_bounds__(NT, 1) k_tl_fused(TileSetDev ts, int B, int cpb, Base<float> bs,
                                                      const float *__restrict__ ut, const float *__restrict__ ht,
                                                      float a, RK<float, double> rku, RK<float, double> rkh,
                                                      int *bad, int early) {
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(256, 2) k_tl_fused(TileSetDev ts, int B, int c
   const TileSmem t = stage_tile(ts, (B / M) / cpb, false);
   const int nEo = t.n[E_OWN], nEm = t.n[E_MID], nEa = t.n[E_ALL], nCo = t.n[C_OWN], nCk = t.n[C_KE],
             nCm = t.n[C_MID], nCa = t.n[C_ALL], nVa = t.n[V_ALL];
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = NT;
   // the linearisation point on the tile (shared by every member)
   float *sUB = reinterpret_cast<float *>(t.rest), *sHB = sUB + nEa, *sPB = sHB + nEa, *sGT = sPB + nEm;
   float *sVB = sGT + nEm, *sGN = sVB + nEm, *sHVB = sGN + nEm, *sVOB = sHVB + nVa;
@@ -324,15 +324,15 @@ __global__ void __launch_bounds__(256, 2) k_tl_fused(TileSetDev ts, int B, int c
 // (src/mpas_sw_dyncore_adj.f90) at one linearisation point, as gathers over the tile, and the
 // adjoint RK bookkeeping (ad_emit).
 // ----------------------------------------------------------------------------------------
-template <int M>
-__global__ void __launch_bounds__(256, 2) k_ad_fused(TileSetDev ts, int B, int cpb, Base<float> bs, float a,
+template <int M, int NT>
+__global__ void __launch_bounds__(NT, 1) k_ad_fused(TileSetDev ts, int B, int cpb, Base<float> bs, float a,
                                                      AdIn<float> in, AdOut<float, double> out, int *bad,
                                                      int early) {
   constexpr int T = M / 4;
   const TileSmem t = stage_tile(ts, (B / M) / cpb, true);
   const int nEo = t.n[E_OWN], nEm = t.n[E_MID], nEa = t.n[E_ALL], nCo = t.n[C_OWN], nCk = t.n[C_KE],
             nCm = t.n[C_MID], nCa = t.n[C_ALL], nVa = t.n[V_ALL];
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = NT;
   float *sUB = reinterpret_cast<float *>(t.rest), *sHB = sUB + nEa, *sPB = sHB + nEa, *sVB = sPB + nEa;
   float *sGT = sVB + nEm, *sGN = sGT + nEm, *sHVB = sGN + nEm, *sVOB = sHVB + nVa;
   F4 *rows = reinterpret_cast<F4 *>(t.rest + 4 * (size_t)base_floats(t.n, true));

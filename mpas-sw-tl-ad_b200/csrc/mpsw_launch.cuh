@@ -16,7 +16,6 @@
 namespace mpsw {
 
 constexpr int kThreads = 128;
-constexpr int kFusedThreads = 256;             // threads of a fused-stage block
 constexpr size_t kFusedSmemMax = 227 * 1024;   // shared memory a block may use
 
 // Grid and block for `total` threads: 128-thread blocks (measured faster than 256 for the
@@ -399,11 +398,27 @@ inline int fused_cpb(int B, int M) {
 template <typename R, typename A>
 bool Launch<R, A>::fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M) {
   constexpr bool f32 = std::is_same<R, float>::value && std::is_same<A, double>::value;
-  if (!f32 || !f.ok || (M != 4 && M != 8) || B % M) return false;
+  if (!f32 || !f.ok || (M != 4 && M != 8 && M != 16) || B % M) return false;
   if (ph.visc2 > R(0) || ph.visc4 > R(0) || ph.wind || ph.drag) return false;
-  const int i = M == 8 ? 1 : 0;
+  const int i = M == 16 ? 2 : M == 8 ? 1 : 0;
   return f.tl.smem[i] <= kFusedSmemMax && f.ad.smem[i] <= kFusedSmemMax;
 }
+
+// run the statement with compile-time MM (members per chunk) and NN (threads per block)
+#define MPSW_FUSED_DISPATCH(M, NT, ...)                                                       \
+  switch ((M) * 10000 + (NT)) {                                                               \
+    case 40256: { constexpr int MM = 4, NN = 256; __VA_ARGS__; } break;                       \
+    case 40512: { constexpr int MM = 4, NN = 512; __VA_ARGS__; } break;                       \
+    case 41024: { constexpr int MM = 4, NN = 1024; __VA_ARGS__; } break;                      \
+    case 80256: { constexpr int MM = 8, NN = 256; __VA_ARGS__; } break;                       \
+    case 80512: { constexpr int MM = 8, NN = 512; __VA_ARGS__; } break;                       \
+    case 81024: { constexpr int MM = 8, NN = 1024; __VA_ARGS__; } break;                      \
+    case 160256: { constexpr int MM = 16, NN = 256; __VA_ARGS__; } break;                     \
+    case 160512: { constexpr int MM = 16, NN = 512; __VA_ARGS__; } break;                     \
+    case 161024: { constexpr int MM = 16, NN = 1024; __VA_ARGS__; } break;                    \
+    default: throw std::invalid_argument("fused stage: unsupported members per chunk or block size"); \
+  }
+
 template <typename R, typename A>
 cudaError_t Launch<R, A>::fused_prepare(const FusedDev &f) {
   if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {
@@ -413,10 +428,11 @@ cudaError_t Launch<R, A>::fused_prepare(const FusedDev &f) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
       if (err == cudaSuccess) err = e;
     };
-    raise((const void *)k_tl_fused<4>, f.tl.smem[0]);
-    raise((const void *)k_tl_fused<8>, f.tl.smem[1]);
-    raise((const void *)k_ad_fused<4>, f.ad.smem[0]);
-    raise((const void *)k_ad_fused<8>, f.ad.smem[1]);
+    for (int M : {4, 8, 16}) {
+      const int i = M == 16 ? 2 : M == 8 ? 1 : 0;
+      MPSW_FUSED_DISPATCH(M, f.nt, raise((const void *)k_tl_fused<MM, NN>, f.tl.smem[i]);
+                          raise((const void *)k_ad_fused<MM, NN>, f.ad.smem[i]));
+    }
     return err;
   } else {
     (void)f;
@@ -432,12 +448,10 @@ void Launch<R, A>::tl_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
     if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused tangent-linear stage not available here");
     g_launches++;
     const float a = ph.apvm * ph.dt;
-    const int cpb = fused_cpb(B, M);
-    const LaunchCfg c{f.tl.ntiles * ((B / M) / cpb), kFusedThreads, f.tl.smem[M == 8]};
-    if (M == 8)
-      launch_k(k_tl_fused<8>, c, s, f.tl, B, cpb, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
-    else
-      launch_k(k_tl_fused<4>, c, s, f.tl, B, cpb, bs, ut, ht, a, rku, rkh, ph.bad, (int)g_stable_base);
+    const int cpb = fused_cpb(B, M), i = M == 16 ? 2 : M == 8 ? 1 : 0;
+    const LaunchCfg c{f.tl.ntiles * ((B / M) / cpb), f.nt, f.tl.smem[i]};
+    MPSW_FUSED_DISPATCH(M, f.nt, launch_k(k_tl_fused<MM, NN>, c, s, f.tl, B, cpb, bs, ut, ht, a, rku, rkh, ph.bad,
+                                          (int)g_stable_base));
   } else {
     throw std::invalid_argument("fused stages run FP32 members only");
   }
@@ -450,12 +464,10 @@ void Launch<R, A>::ad_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
     if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused adjoint stage not available here");
     g_launches++;
     const float a = ph.apvm * ph.dt;
-    const int cpb = fused_cpb(B, M);
-    const LaunchCfg c{f.ad.ntiles * ((B / M) / cpb), kFusedThreads, f.ad.smem[M == 8]};
-    if (M == 8)
-      launch_k(k_ad_fused<8>, c, s, f.ad, B, cpb, bs, a, in, out, ph.bad, (int)g_stable_base);
-    else
-      launch_k(k_ad_fused<4>, c, s, f.ad, B, cpb, bs, a, in, out, ph.bad, (int)g_stable_base);
+    const int cpb = fused_cpb(B, M), i = M == 16 ? 2 : M == 8 ? 1 : 0;
+    const LaunchCfg c{f.ad.ntiles * ((B / M) / cpb), f.nt, f.ad.smem[i]};
+    MPSW_FUSED_DISPATCH(M, f.nt, launch_k(k_ad_fused<MM, NN>, c, s, f.ad, B, cpb, bs, a, in, out, ph.bad,
+                                          (int)g_stable_base));
   } else {
     throw std::invalid_argument("fused stages run FP32 members only");
   }

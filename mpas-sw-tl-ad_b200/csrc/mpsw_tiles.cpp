@@ -312,7 +312,7 @@ static size_t tile_smem(const int *cnt, bool adjoint, int M) {
          (size_t)member_rows(cnt, adjoint) * M * sizeof(float);
 }
 
-std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, bool adjoint, TileSetHost *o) {
+std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, int M, bool adjoint, TileSetHost *o) {
   if (kmax < 1) return "tile size must be positive";
   for (int c = 0; c < m.nC; c++)
     if (m.c_n[c] > kCellSlots) return "fused tiles need at most 6 edges per cell";
@@ -322,12 +322,12 @@ std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, bool adjoin
   const int nC = m.nC;
   int stamp = 0;  // a fresh id for each trial build of the spaces
   int cnt[kTileCounts];
-  // shared memory of the tile [c0, c1) with 4 members per chunk
+  // shared memory of the tile [c0, c1) with M members per chunk
   auto fits = [&](int c0, int c1) {
     Space E(b.se, b.le, stamp), C(b.sc, b.lc, stamp), V(b.sv, b.lv, stamp);
     stamp++;
     tile_spaces(b, m, c0, c1, adjoint, E, C, V, cnt);
-    return tile_smem(cnt, adjoint, 4) <= budget && E.list.size() < kNoLocal && C.list.size() < kNoLocal &&
+    return tile_smem(cnt, adjoint, M) <= budget && E.list.size() < kNoLocal && C.list.size() < kNoLocal &&
            V.list.size() < kNoLocal;
   };
   // partition the cells into runs of the internal order: each run as long as its tile's shared
@@ -377,7 +377,7 @@ std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, bool adjoin
     o->gv.insert(o->gv.end(), V.list.begin(), V.list.end());
     o->blob_off[t] = (long long)o->blob.size();
     pack_blob(b, m, E, C, V, tc, adjoint, &o->blob);
-    for (int i = 0; i < 2; i++) o->smem[i] = std::max(o->smem[i], tile_smem(tc, adjoint, 4 << i));
+    for (int i = 0; i < 3; i++) o->smem[i] = std::max(o->smem[i], tile_smem(tc, adjoint, 4 << i));
   }
   return "";
 }

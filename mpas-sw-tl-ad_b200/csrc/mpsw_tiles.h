@@ -44,15 +44,15 @@ struct TileSetHost {
   std::vector<int> ge, gc, gv;              // internal index of each local entity, tile after tile
   std::vector<unsigned char> blob;          // the tiles' blobs (BlobSection), each 16-byte aligned
   std::vector<long long> blob_off;          // [ntiles] byte offset of each tile's blob
-  size_t smem[2] = {0, 0};                  // shared memory of the stage's block, 4 / 8 members
+  size_t smem[3] = {0, 0, 0};               // shared memory of the stage's block, 4 / 8 / 16 members
 };
 
 // Build the tangent-linear (adjoint = false) or adjoint tiles for a mesh with at most 6 edges
 // per cell and 10 edgesOnEdge, with their blobs (coefficients formed in FP64 from the mesh and
 // rounded to FP32).  Each tile owns a run of consecutive cells of the internal order, as long as
-// its block's shared memory with 4 members per chunk stays within `budget` bytes and at most
+// its block's shared memory with M members per chunk stays within `budget` bytes and at most
 // `kmax` cells.  Returns an empty string or the problem found (a cell whose halo alone exceeds
 // the budget, or a phase that would read outside its tile).
-std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, bool adjoint, TileSetHost *out);
+std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, int M, bool adjoint, TileSetHost *out);
 
 }  // namespace mpsw

@@ -491,18 +491,17 @@ void Engine::window_ensure() {
   if (win.pending) window_forward();
 }
 
-// Members per block of the fused stage kernels for B members of precision R (0: the split
-// member kernels run instead: FP64 members, physics beyond the fused kernels, or MPSW_FUSED=0).
-// MPSW_FUSED_M=4|8 chooses the chunk; the default is 4 (the smaller shared-memory footprint).
+// Members per chunk of the fused stage kernels for B members of precision R (0: the split member
+// kernels run instead: FP64 members, physics beyond the fused kernels, or no fused tiles).
 template <typename R>
 static int fused_members(const Engine &E, int B, const Phys<R> &ph) {
   if constexpr (std::is_same<R, double>::value) {
     return 0;
   } else {
-    const char *env = getenv("MPSW_FUSED_M");
-    const int forced = env ? atoi(env) : 0;
-    const int M = forced == 4 || forced == 8 ? forced : 4;
-    return Launch<R, double>::fused_ok(E.fused, B, ph, M) ? M : 0;
+    // the chunk the tiles were sized for, else the largest smaller one B is a multiple of
+    for (int M = E.fused.M; M >= 4; M /= 2)
+      if (Launch<R, double>::fused_ok(E.fused, B, ph, M)) return M;
+    return 0;
   }
 }
 

@@ -85,20 +85,20 @@ def test_fused_independent_of_tile_size_and_storage():
             assert torch.equal(a, b)
 
 
-def test_fused_members_per_block():
+@pytest.mark.parametrize('nt', ['256', '1024'])
+def test_fused_members_per_chunk_and_block_size(nt):
+    """Chunks of 4, 8 and 16 members and blocks of 256 or 1024 threads give the same results (the
+    chunk changes only which members a thread holds; FP32 contraction may differ per build)."""
     from mpsw.torch_api import FP32
     B = 16
-    m, e = engine(4, {'MPSW_FUSED': '1'})
-    du, dh = members(m, B, 5)
-    yu, yh = members(m, B, 6)
     res = []
-    for M in ('4', '8'):
-        os.environ['MPSW_FUSED_M'] = M
-        try:
-            res.append(sweep(e, du, dh, yu, yh, FP32))
-        finally:
-            os.environ.pop('MPSW_FUSED_M', None)
+    for M in ('4', '8', '16'):
+        m, e = engine(4, {'MPSW_FUSED': '1', 'MPSW_FUSED_M': M, 'MPSW_FUSED_NT': nt})
+        du, dh = members(m, B, 5)
+        yu, yh = members(m, B, 6)
+        res.append(sweep(e, du, dh, yu, yh, FP32))
     assert relmax(res[0], res[1]) < 1e-6
+    assert relmax(res[0], res[2]) < 1e-6
 
 
 def test_split_kernels_serve_other_physics():

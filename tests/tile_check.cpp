@@ -10,8 +10,8 @@
 using namespace mpsw;
 
 // out[0] tiles, out[1] owned cells summed over tiles, out[2] owned edges summed, out[3] cells
-// owned twice or never, out[4] edges owned twice or never, out[5] shared-memory bytes (M = 4),
-// out[6] (M = 8); returns 0 or 1 with the builder's message in err.
+// owned twice or never, out[4] edges owned twice or never, out[5] shared-memory bytes (M = 4,
+// the tiles' budget), out[6] (M = 8); returns 0 or 1 with the builder's message in err.
 extern "C" int tile_check(int nC, int nE, int nV, int maxEdges, int maxEdges2, const int *coe, const int *voe,
                           const int *eoe, const int *neoe, const int *eoc, const int *neoc, const int *cov,
                           const int *eov, const double *w, const double *kites, const double *dc,
@@ -32,7 +32,7 @@ extern "C" int tile_check(int nC, int nE, int nV, int maxEdges, int maxEdges2, c
   BuiltMesh bm;
   std::string e = build_mesh(r, g, 1, &bm);
   TileSetHost t;
-  if (e.empty()) e = build_tiles(bm, (size_t)budget_kb << 10, K, adjoint != 0, &t);
+  if (e.empty()) e = build_tiles(bm, (size_t)budget_kb << 10, K, 4, adjoint != 0, &t);
   if (!e.empty()) {
     std::strncpy(err, e.c_str(), errlen - 1);
     err[errlen - 1] = 0;
