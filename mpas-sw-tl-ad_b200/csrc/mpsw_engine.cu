@@ -413,7 +413,7 @@ void Engine::free_device_mesh() {
 // Halo tiles of the fused FP32 member stages (meshes with at most 6 edges per cell and 10
 // edgesOnEdge), built when MPSW_FUSED=1 is set as the mesh goes to the device (the sweeps use
 // the split member kernels otherwise).  MPSW_FUSED_M sets the members per chunk the tiles are
-// sized for (4, 8 or 16; default 8), MPSW_FUSED_NT the threads per block (256, 512 or 1024;
+// sized for (4, 8, 16 or 32; default 8), MPSW_FUSED_NT the threads per block (256, 512 or 1024;
 // default 512), MPSW_FUSED_SMEM the shared memory of a tile's block in KB (default 110) and
 // MPSW_FUSED_K the most cells a tile owns (default 1024).
 void Engine::build_fused() {
@@ -428,7 +428,7 @@ void Engine::build_fused() {
   };
   const int K = env("MPSW_FUSED_K", 1024), M = env("MPSW_FUSED_M", 8), NT = env("MPSW_FUSED_NT", 512);
   const size_t budget = (size_t)env("MPSW_FUSED_SMEM", 110) << 10;
-  if (M != 4 && M != 8 && M != 16) throw EngineError(MPSW_ERR_ARG, "MPSW_FUSED_M must be 4, 8 or 16");
+  if (M != 4 && M != 8 && M != 16 && M != 32) throw EngineError(MPSW_ERR_ARG, "MPSW_FUSED_M must be 4, 8, 16 or 32");
   if (NT != 256 && NT != 512 && NT != 1024) throw EngineError(MPSW_ERR_ARG, "MPSW_FUSED_NT must be 256, 512 or 1024");
   TileSetHost th[2];
   for (int a = 0; a < 2; a++) {
@@ -443,7 +443,7 @@ void Engine::build_fused() {
     d.cnt = up<int>(t.cnt, o);
     d.blob_off = up<long long>(t.blob_off, o);
     d.blob = up<unsigned char>(t.blob, o);
-    for (int i = 0; i < 3; i++) d.smem[i] = t.smem[i];
+    for (int i = 0; i < 4; i++) d.smem[i] = t.smem[i];
   }
   fused.M = M;
   fused.nt = NT;

@@ -221,12 +221,12 @@ struct TileSetDev {
   const int *cnt = nullptr;
   const long long *blob_off = nullptr;
   const unsigned char *blob = nullptr;
-  size_t smem[3] = {0, 0, 0};  // dynamic shared memory of a block for 4, 8 and 16 members per chunk
+  size_t smem[4] = {0, 0, 0, 0};  // dynamic shared memory of a block for 4, 8, 16, 32 members per chunk
 };
 
 struct FusedDev {
   bool ok = false;  // tiles built (meshes within 6 edgesOnCell, 10 edgesOnEdge)
-  int M = 8;        // members per chunk the tiles were sized for (4, 8 or 16)
+  int M = 8;        // members per chunk the tiles were sized for (4, 8, 16 or 32)
   int nt = 512;     // threads per block (256, 512 or 1024)
   TileSetDev tl, ad;
 };

@@ -389,6 +389,7 @@ void Launch<R, A>::ad_part(int which, const MeshDev<R> &m, int B, const Base<R> 
 // Chunks of M members one fused-stage block walks (all B / M of its tile by default; fewer
 // blocks per tile take more chunks each, so the tile's blob is staged fewer times).
 // MPSW_FUSED_CPB overrides it when it divides B / M.
+inline int fused_smem_index(int M) { return M == 32 ? 3 : M == 16 ? 2 : M == 8 ? 1 : 0; }
 inline int fused_cpb(int B, int M) {
   const int chunks = B / M;
   const char *e = std::getenv("MPSW_FUSED_CPB");
@@ -398,9 +399,10 @@ inline int fused_cpb(int B, int M) {
 template <typename R, typename A>
 bool Launch<R, A>::fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M) {
   constexpr bool f32 = std::is_same<R, float>::value && std::is_same<A, double>::value;
-  if (!f32 || !f.ok || (M != 4 && M != 8 && M != 16) || B % M) return false;
+  if (!f32 || !f.ok || (M != 4 && M != 8 && M != 16 && M != 32) || B % M) return false;
   if (ph.visc2 > R(0) || ph.visc4 > R(0) || ph.wind || ph.drag) return false;
-  const int i = M == 16 ? 2 : M == 8 ? 1 : 0;
+  if (M == 32 && f.nt == 256) return false;  // 32 members per chunk: 512- or 1024-thread blocks
+  const int i = fused_smem_index(M);
   return f.tl.smem[i] <= kFusedSmemMax && f.ad.smem[i] <= kFusedSmemMax;
 }
 
@@ -416,6 +418,8 @@ bool Launch<R, A>::fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M) 
     case 160256: { constexpr int MM = 16, NN = 256; __VA_ARGS__; } break;                     \
     case 160512: { constexpr int MM = 16, NN = 512; __VA_ARGS__; } break;                     \
     case 161024: { constexpr int MM = 16, NN = 1024; __VA_ARGS__; } break;                    \
+    case 320512: { constexpr int MM = 32, NN = 512; __VA_ARGS__; } break;                     \
+    case 321024: { constexpr int MM = 32, NN = 1024; __VA_ARGS__; } break;                    \
     default: throw std::invalid_argument("fused stage: unsupported members per chunk or block size"); \
   }
 
@@ -428,8 +432,9 @@ cudaError_t Launch<R, A>::fused_prepare(const FusedDev &f) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
       if (err == cudaSuccess) err = e;
     };
-    for (int M : {4, 8, 16}) {
-      const int i = M == 16 ? 2 : M == 8 ? 1 : 0;
+    for (int M : {4, 8, 16, 32}) {
+      if (M == 32 && f.nt == 256) continue;
+      const int i = fused_smem_index(M);
       MPSW_FUSED_DISPATCH(M, f.nt, raise((const void *)k_tl_fused<MM, NN>, f.tl.smem[i]);
                           raise((const void *)k_ad_fused<MM, NN>, f.ad.smem[i]));
     }
@@ -448,7 +453,7 @@ void Launch<R, A>::tl_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
     if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused tangent-linear stage not available here");
     g_launches++;
     const float a = ph.apvm * ph.dt;
-    const int cpb = fused_cpb(B, M), i = M == 16 ? 2 : M == 8 ? 1 : 0;
+    const int cpb = fused_cpb(B, M), i = fused_smem_index(M);
     const LaunchCfg c{f.tl.ntiles * ((B / M) / cpb), f.nt, f.tl.smem[i]};
     MPSW_FUSED_DISPATCH(M, f.nt, launch_k(k_tl_fused<MM, NN>, c, s, f.tl, B, cpb, bs, ut, ht, a, rku, rkh, ph.bad,
                                           (int)g_stable_base));
@@ -464,7 +469,7 @@ void Launch<R, A>::ad_fused(const FusedDev &f, int M, const MeshDev<R> &m, int B
     if (!fused_ok(f, B, ph, M)) throw std::invalid_argument("fused adjoint stage not available here");
     g_launches++;
     const float a = ph.apvm * ph.dt;
-    const int cpb = fused_cpb(B, M), i = M == 16 ? 2 : M == 8 ? 1 : 0;
+    const int cpb = fused_cpb(B, M), i = fused_smem_index(M);
     const LaunchCfg c{f.ad.ntiles * ((B / M) / cpb), f.nt, f.ad.smem[i]};
     MPSW_FUSED_DISPATCH(M, f.nt, launch_k(k_ad_fused<MM, NN>, c, s, f.ad, B, cpb, bs, a, in, out, ph.bad,
                                           (int)g_stable_base));

@@ -377,7 +377,7 @@ std::string build_tiles(const BuiltMesh &m, size_t budget, int kmax, int M, bool
     o->gv.insert(o->gv.end(), V.list.begin(), V.list.end());
     o->blob_off[t] = (long long)o->blob.size();
     pack_blob(b, m, E, C, V, tc, adjoint, &o->blob);
-    for (int i = 0; i < 3; i++) o->smem[i] = std::max(o->smem[i], tile_smem(tc, adjoint, 4 << i));
+    for (int i = 0; i < 4; i++) o->smem[i] = std::max(o->smem[i], tile_smem(tc, adjoint, 4 << i));
   }
   return "";
 }

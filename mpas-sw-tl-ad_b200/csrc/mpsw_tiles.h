@@ -44,7 +44,7 @@ struct TileSetHost {
   std::vector<int> ge, gc, gv;              // internal index of each local entity, tile after tile
   std::vector<unsigned char> blob;          // the tiles' blobs (BlobSection), each 16-byte aligned
   std::vector<long long> blob_off;          // [ntiles] byte offset of each tile's blob
-  size_t smem[3] = {0, 0, 0};               // shared memory of the stage's block, 4 / 8 / 16 members
+  size_t smem[4] = {0, 0, 0, 0};            // shared memory of the stage's block, 4 / 8 / 16 / 32 members
 };
 
 // Build the tangent-linear (adjoint = false) or adjoint tiles for a mesh with at most 6 edges
