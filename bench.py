@@ -1,7 +1,8 @@
 """Benchmark: tangent-linear + adjoint gradients per second of the MPAS shallow-water RK4 model.
 
 Workload (default): level-7 bisected-icosahedron TRiSK mesh (163842 cells, 491520 edges, 327680
-vertices), seeded balanced flow (seed 0), dt = 75 s, a 288-step (6 h) window, trajectory
+vertices), seeded balanced flow (seed 0) over 8 seeded mountains (h reduced by the
+topography), dt = 75 s, a 288-step (6 h) window, trajectory
 checkpointed every 16 steps, perturbations h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s), B = 64 members.  One bench step
 is one gradient batch: the nonlinear window with checkpoints, the B-member tangent-linear
 sweep and the B-member adjoint sweep (seeded with the tangent-linear output, i.e. the gradient
@@ -111,15 +112,15 @@ def perturbations(unit, B, seed=1):
 
 # ---- reference arm and CPU baseline: the oracle (serial C restatement of the Fortran) -------
 class OracleMember:
-    """One member's oracle instance on the host: the workload's mesh, balanced flow and a seeded
-    perturbation, built once; sample(n) times n forward, n tangent-linear and n adjoint steps."""
+    """One member's oracle instance on the host: the workload's mesh, balanced flow over
+    mountains and a seeded perturbation, built once; sample(n) times n forward, n
+    tangent-linear and n adjoint steps."""
 
     def __init__(self, level, dt, seed):
         sys.path.insert(0, os.path.join(ROOT, 'oracle'))
         import oracle as O
-        unit, mesh, st = workload(level, dt)
         m = O.OracleModule()
-        load_module(m, unit, mesh, st, dt)
+        unit = forward_module(m, level, dt)
         m.var_allocation_tlm()
         m.var_allocation_adj()
         m.sw_mpas_init_block()
@@ -230,7 +231,7 @@ def run_reference(a, rank, world):
         'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': a.gpus,
         'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': ms,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
-        'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh)' % a.level,
+        'data': 'synthetic (seeded balanced flow over 8 seeded mountains, level-%d TRiSK mesh)' % a.level,
         'config': workload_config(a),
         'sample_ms': [round(1e3 * w, 1) for w in walls],
         'extrapolation': {'steps_per_sample': 1, 'window_steps': a.nsteps,
@@ -430,9 +431,8 @@ def run_mpsw(a, rank, world):
 
     dev = rank % max(1, torch.cuda.device_count())
     torch.cuda.set_device(dev)
-    unit, mesh, st = workload(a.level, a.dt)
     mod = MpasSwModule()
-    load_module(mod, unit, mesh, st, a.dt)
+    unit = forward_module(mod, a.level, a.dt)
     mod.var_allocation_tlm()
     mod.var_allocation_adj()
     mod.sw_mpas_init_block()
@@ -619,7 +619,7 @@ def run_mpsw(a, rank, world):
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': a.steps,
             'warmup': a.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f32 stencils + f64 accumulation',
-            'data': 'synthetic (seeded balanced flow, level-%d TRiSK mesh, seeded perturbations)' % a.level,
+            'data': 'synthetic (seeded balanced flow over 8 seeded mountains, level-%d TRiSK mesh, seeded perturbations)' % a.level,
             'config': workload_config(a),
             'stage_storage': {-1: 'auto (FP64+FP32 stage linearisation points when they fit 40%% of free HBM)', 0: 'none: stages recomputed from checkpoints', 1: 'FP64', 2: 'FP32', 3: 'FP64+FP32'}[a.storage],
             'working_set_mb': round(wset),
