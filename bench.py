@@ -1,12 +1,11 @@
 """Benchmark: tangent-linear + adjoint gradients per second of the MPAS shallow-water RK4 model.
 
 Workload (default): level-7 bisected-icosahedron TRiSK mesh (163842 cells, 491520 edges, 327680
-vertices), seeded balanced flow (seed 0) over 8 seeded mountains (h reduced by the
-topography), dt = 75 s, a 288-step (6 h) window, trajectory
-checkpointed every 16 steps, perturbations h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s), B = 64 members.  One bench step
-is one gradient batch: the nonlinear window with checkpoints, the B-member tangent-linear
-sweep and the B-member adjoint sweep (seeded with the tangent-linear output, i.e. the gradient
-of 1/2 |L dx|^2).  `value` counts gradients of the batched FP32-stencil / FP64-accumulation
+vertices), seeded balanced flow (seed 0) over 8 seeded mountains (h reduced by the topography),
+dt = 75 s, a 288-step (6 h) window, trajectory checkpointed every 16 steps, perturbations
+h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s), B = 64 members.  One bench step is one gradient batch:
+the nonlinear window with checkpoints, the B-member tangent-linear sweep and the B-member
+adjoint sweep (seeded with the tangent-linear output, i.e. the gradient of 1/2 |L dx|^2).  `value` counts gradients of the batched FP32-stencil / FP64-accumulation
 form; the plain FP64 single-member form is timed beside it, with the relative L2 error of the
 batched result against the FP64 window.
 
@@ -337,7 +336,8 @@ class Clocks:
 # ---- algorithmic bytes of the member kernels ------------------------------------------------------
 def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
     """Bytes a launch must move if every array element it touches is read or written once
-    (viscosity, drag and wind off, as in the benchmark workload).
+    (viscosity, drag and wind off, as in the benchmark workload: the sweeps then neither write
+    divergence' / vorticity' nor form divergence_ad, which feed only the viscosity terms).
 
     s: bytes of a member value, a linearisation-point value and a mesh metric (4 in FP32);
     accumulators and member RK states are a = 8 bytes; connectivity words 4 bytes, edge signs
@@ -350,10 +350,10 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
     kb = {
         'tl_vertex': (3 * i + 3 + 3 * i + 3 * s) * V + 2 * s * V + s * E   # v_es,esg,v_c,kites; area,f; dc
                      + 2 * s * V                                          # base h_vertex, vorticity
-                     + B * s * (E + C + 2 * V),                           # u,h in; vort, pv out
+                     + B * s * (E + C + V),                               # u,h in; pv out
         'tl_cell': (i + 3 * 6 * i + 6 + 6 * s + s) * C + (2 * i + 2 * s) * E  # c_n,es,eoc,vs,esg,kites,area; c1,c2,dc,dv
                    + 2 * s * E                                                  # base u, h_edge
-                   + B * (s * (E + C + V + 3 * C) + (a + 2 * s) * C),          # u,h,pv in; div,ke,pc out; RK
+                   + B * (s * (E + C + V + 2 * C) + (a + 2 * s) * C),          # u,h,pv in; ke,pc out; RK
         'tl_edge_diag': eoe + (6 * i + 2 * s) * E + 4 * s * E                  # ends; dc,dv; base gradPVt,v,gradPVn,u
                         + (2 * s * E if s == 4 else 0)                         # FP32: base h_edge, pv_edge
                         + B * s * (E + C + V + C + 2 * E)                      # u,h,pv,pc in; pv_edge,h_edge out
@@ -363,11 +363,11 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
         'ad_edge': eoe + s * S + (2 * i + s) * E + 6 * s * E                   # wrev; c1,c2,dv; 6 base fields
                    + B * s * (E + C + 3 * E),                                  # tu,th in; pe_ad,he_ad,ud out
         'ad_cell': (i + 6 * i + 6 + s) * C + 2 * s * E                         # c_n,es,esg,area; dc; base u
-                   + B * s * (3 * E + 4 * C),                                  # tu,pe_ad,he_ad in; 4 out
+                   + B * s * (3 * E + 3 * C),                                  # tu,pe_ad,he_ad in; 3 out
         'ad_vertex': (3 * i + 3 * s + 3 * i + 3 * i + 3 + 2 * s) * V + s * C + 2 * s * E + 2 * s * V
                      + B * s * (C + E + 2 * V),                                # pc_ad,pe_ad in; 2 out
         'ad_final': (i + 6 * i + 6 * s + s) * C + i * (E + S) + s * S + (4 * i + 2 * s) * E + 2 * s * E
-                    + B * (s * (2 * C + 2 * V + 2 * E + C) + (a + 2 * s) * (C + E)),
+                    + B * (s * (C + 2 * V + 2 * E + C) + (a + 2 * s) * (C + E)),
     }
     kb['tl_stage'] = sum(kb[k] for k in ('tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend'))
     kb['ad_stage'] = sum(kb[k] for k in ('ad_edge', 'ad_cell', 'ad_vertex', 'ad_final'))

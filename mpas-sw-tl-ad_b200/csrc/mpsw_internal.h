@@ -112,6 +112,9 @@ struct RK {
   R *t_out;
   const R *t_in[3];
   A wt[3];
+  // FP32 members: the step's input rounded to R; when set, stages 1-3 form the next provisional
+  // state as x0r + c t in R instead of reading the FP64 state x0
+  const R *x0r;
 };
 
 // Input of one adjoint stage: its tendency adjoint, tu (edges) and th / areaCell (cells), as
@@ -159,6 +162,10 @@ struct AdOut {
   // contributions in stage order before adding x2 and its own: the same FP64 operations.
   R *pad_out_u, *pad_out_h;
   const R *pad_in_u[3], *pad_in_h[3];
+  // FP32 members: x2 rounded to R.  When set, AD_SET / AD_ADD stages form tu_next / th_next from
+  // it (four bytes a value instead of x2's eight), and AD_FINAL writes the rounding of its dst
+  // there for the step before.
+  R *x2r_u, *x2r_h;
 };
 
 // ---- fused member stages (mpsw_fused.cuh, tiles built by mpsw_tiles.cpp) ----------------

@@ -95,10 +95,17 @@ template <typename R, typename A, int V>
 __device__ __forceinline__ void rk_members(const RK<R, A> &rk, size_t o, const Mv<R, V> &t) {
   const bool last = rk.t_in[0] != nullptr;  // the stage that sums the stored tendencies
   if (rk.next && !last) {
-    const Mv<A, V> x0 = ldv<V>(rk.x0 + o);
     Mv<R, V> n;
+    if (rk.x0r) {
+      const Mv<R, V> x = ldv<V>(rk.x0r + o);
+      const R c = R(rk.c);
 #pragma unroll
-    for (int i = 0; i < V; i++) n.x[i] = rk.frozen ? R(x0.x[i]) : R(x0.x[i] + rk.c * A(t.x[i]));
+      for (int i = 0; i < V; i++) n.x[i] = x.x[i] + c * t.x[i];
+    } else {
+      const Mv<A, V> x0 = ldv<V>(rk.x0 + o);
+#pragma unroll
+      for (int i = 0; i < V; i++) n.x[i] = rk.frozen ? R(x0.x[i]) : R(x0.x[i] + rk.c * A(t.x[i]));
+    }
     stv<V>(rk.next + o, n);
   }
   if (rk.frozen) return;
@@ -297,7 +304,7 @@ __global__ void k_tl_vertex(MeshDev<R> m, int B, Base<R> bs, const R *__restrict
     const M pvt = vort / hv - (hvt * (ld(m.v_f, v) + ld(bs.vort, v))) / (hv * hv);
     const size_t o = (size_t)v * B + q.b;
     if (d.circ) stv<V>(d.circ + o, circ);
-    stv<V>(d.vort + o, vort);
+    if (d.vort) stv<V>(d.vort + o, vort);
     if (d.hv) stv<V>(d.hv + o, hvt);
     stv<V>(d.pvv + o, pvt);
   }
@@ -368,7 +375,7 @@ __global__ void k_tl_vertex_st(MeshDev<R> m, int B, Base<R> bs, const R *__restr
   }
   const size_t o = (size_t)v * B + b;
   if (d.circ) stv<V>(d.circ + o, circ);
-  stv<V>(d.vort + o, vort);
+  if (d.vort) stv<V>(d.vort + o, vort);
   if (d.hv) stv<V>(d.hv + o, hvt);
   stv<V>(d.pvv + o, pvt);
 }
@@ -414,7 +421,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_tl_cell(MeshDev
     }
     th = th / area;
     const size_t o = (size_t)c * B + q.b;
-    stv<V>(d.div + o, div);
+    if (d.div) stv<V>(d.div + o, div);
     stv<V>(d.ke + o, ke);
     stv<V>(d.pc + o, pc);
     if (d.vc) stv<V>(d.vc + o, vc);
@@ -523,7 +530,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
     th = th / area;
   }
   const size_t o = (size_t)c * B + b;
-  stv<V>(d.div + o, div);
+  if (d.div) stv<V>(d.div + o, div);
   stv<V>(d.ke + o, ke);
   stv<V>(d.pc + o, pc);
   if (d.vc) stv<V>(d.vc + o, vc);
@@ -933,7 +940,7 @@ __global__ void k_ad_cell(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
     const size_t o = (size_t)c * B + q.b;
     stv<V>(w.pc_ad + o, pc_ad);
     stv<V>(w.ke_ad + o, ke_ad / area);
-    stv<V>(w.div_ad + o, div_ad * (R(1) / area));
+    if (w.div_ad) stv<V>(w.div_ad + o, div_ad * (R(1) / area));
     stv<V>(w.hd + o, hd);
   }
 }
@@ -1021,7 +1028,7 @@ __global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R
   const size_t o = (size_t)c * B + b;
   stv<V>(w.pc_ad + o, pc_ad);
   stv<V>(w.ke_ad + o, ke_ad / area);
-  stv<V>(w.div_ad + o, div_ad * (R(1) / area));
+  if (w.div_ad) stv<V>(w.div_ad + o, div_ad * (R(1) / area));
   stv<V>(w.hd + o, hd);
 }
 
@@ -1193,6 +1200,7 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
       next.x[i] = wn * d.x[i];
     }
     stv<V>(dst + o, d);
+    if (R *xr = is_edge ? out.x2r_u : out.x2r_h) stv<V>(xr + o, mv_cast<V, R>(d));
   } else {
     if (pout) {
       stv<V>(pout + o, pad);
@@ -1208,9 +1216,16 @@ __device__ __forceinline__ void ad_emit(const AdOut<R, A> &out, int is_edge, siz
       stv<V>(acc + o, a);
     }
     if (tn) {
-      const Mv<A, V> x = x2 ? ldv<V>(x2 + o) : mv_fill<A, V>(A(0));
+      const R *xr = is_edge ? out.x2r_u : out.x2r_h;
+      if (xr) {
+        const Mv<R, V> x = ldv<V>(xr + o);
 #pragma unroll
-      for (int i = 0; i < V; i++) next.x[i] = (x2 ? wn * x.x[i] : A(0)) + cn * A(pad.x[i]);
+        for (int i = 0; i < V; i++) next.x[i] = wn * A(x.x[i]) + cn * A(pad.x[i]);
+      } else {
+        const Mv<A, V> x = x2 ? ldv<V>(x2 + o) : mv_fill<A, V>(A(0));
+#pragma unroll
+        for (int i = 0; i < V; i++) next.x[i] = (x2 ? wn * x.x[i] : A(0)) + cn * A(pad.x[i]);
+      }
     }
   }
   if (tn) {
@@ -1260,8 +1275,10 @@ __device__ __forceinline__ void ad_final_edge(const MeshDev<R> &m, int B, const 
   const R kc = (((R(0.25) * dc) * dv) * R(2)) * ld(bs.u, e);
   pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c1 * B + b);
   pu = pu + kc * ldv<V>(w.ke_ad + (size_t)c2 * B + b);
-  pu = pu - dv * ldv<V>(w.div_ad + (size_t)c2 * B + b);
-  pu = pu + dv * ldv<V>(w.div_ad + (size_t)c1 * B + b);
+  if (w.div_ad) {  // null where it would be zero (window sweeps without viscosity)
+    pu = pu - dv * ldv<V>(w.div_ad + (size_t)c2 * B + b);
+    pu = pu + dv * ldv<V>(w.div_ad + (size_t)c1 * B + b);
+  }
   pu = pu + dc * ldv<V>(w.circ_ad + (size_t)v2 * B + b);
   pu = pu - dc * ldv<V>(w.circ_ad + (size_t)v1 * B + b);
   if (ph.bad) {

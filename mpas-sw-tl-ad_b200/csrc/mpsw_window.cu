@@ -31,7 +31,11 @@ using L64 = Launch<double, double>;
 template <typename R>
 struct MemberBufs {
   Diag<R> d{};
-  R *pu[3] = {}, *ph[3] = {};
+  // tangent-linear provisional states of stages 2-4 (pu / ph [0..2]) and, for FP32 members, the
+  // step's rounded input state (pu / ph [3]): the tangent-linear members', which stages 1-3 form
+  // their provisional states from, or in adjoint sweeps the adjoint state's, which stages 4-2
+  // form the next tendency adjoint from
+  R *pu[4] = {}, *ph[4] = {};
   AdWork<R> w{};
   R *pad_u[2] = {}, *pad_h[2] = {};
   // per-stage tendencies (tangent linear) or contributions (adjoint) of the first three stages
@@ -76,7 +80,7 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   // FP32 members keep the tangent PV flux in d.v (read by tl_edge_tend); FP64 needs no v'
   d.v = sizeof(R) == 4 ? walloc<R>(M, Ed, s) : nullptr;
   d.dsq_u = walloc<R>(M, Ed, s); d.dsq_vort = walloc<R>(M, V, s); d.dsq_div = walloc<R>(M, C, s);
-  for (int k = 0; k < 3; k++) {
+  for (int k = 0; k < 4; k++) {
     mb->pu[k] = walloc<R>(M, Ed, s);
     mb->ph[k] = walloc<R>(M, C, s);
   }
@@ -103,6 +107,22 @@ MemberBufs<R> *members(Engine &E, int prec, int B, cudaStream_t s) {
   M.bufs = mb;
   M.B = B;
   return mb;
+}
+
+// The member rows a window sweep passes between its kernels.  divergence' and vorticity' feed
+// only the del2 / del4 terms, and divergence_ad is zero without them (the sweeps have no
+// diagnostic seeds), so without viscosity the kernels neither write nor read those rows.
+template <typename R>
+Diag<R> tl_rows(const MemberBufs<R> *mb, const Phys<R> &ph) {
+  Diag<R> d = mb->d;
+  if (!(ph.visc2 > R(0)) && !(ph.visc4 > R(0))) d.div = d.vort = nullptr;
+  return d;
+}
+template <typename R>
+AdWork<R> ad_rows(const MemberBufs<R> *mb, const Phys<R> &ph) {
+  AdWork<R> w = mb->w;
+  if (!(ph.visc2 > R(0)) && !(ph.visc4 > R(0))) w.div_ad = nullptr;
+  return w;
 }
 
 Base<double> base64(const Window &W, int k) {
@@ -508,10 +528,12 @@ static int fused_members(const Engine &E, int B, const Phys<R> &ph) {
 // Member work of tangent-linear stage k about the linearisation point bs.
 //
 // Stage 1 reads the FP64 member state directly when R is double; otherwise its FP32 rounding in
-// pu[1] / ph[1], made here when `round_in` (the first step of a sweep, or every step where the
+// pu[3] / ph[3], made here when `round_in` (the first step of a sweep, or every step where the
 // previous one did not leave it: per-step graphs, test case 1's frozen wind) and otherwise
-// written by the previous step's stage 4 as it formed the new state.  pu[1] / ph[1] are free
-// then: stage 2 overwrites them after stage 1, stage 4 writes them after stage 3 read them.
+// written by the previous step's stage 4 as it formed the new state.  FP32 members then form the
+// provisional states of stages 2-4 from that rounded input (x + c dt tend in FP32: four bytes a
+// value instead of the FP64 state's eight); the FP64 state is read only by stage 4, which
+// accumulates the step.
 template <typename R>
 static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, MemberBufs<R> *mb,
                             const Phys<R> &ph, const double w[4], const double c[4], int k, const Base<R> &bs,
@@ -527,22 +549,26 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
       hti = dh;
     } else {
       if (round_in || ph.tc1) {
-        convert_d2f((long long)E.nE * B, du, mb->pu[1], st);
-        convert_d2f((long long)E.nC * B, dh, mb->ph[1], st);
+        convert_d2f((long long)E.nE * B, du, mb->pu[3], st);
+        convert_d2f((long long)E.nC * B, dh, mb->ph[3], st);
       }
-      uti = mb->pu[1];
-      hti = mb->ph[1];
+      uti = mb->pu[3];
+      hti = mb->ph[3];
     }
   }
   // stages 1-3 keep their tendencies; stage 4 sums them into the FP64 members (deferred RK4
   // accumulation, the same FP64 additions as accumulating stage by stage)
-  R *nu = k < 3 ? mb->pu[k] : (hand_on ? mb->pu[1] : nullptr);
-  R *nh = k < 3 ? mb->ph[k] : (hand_on ? mb->ph[1] : nullptr);
+  R *nu = k < 3 ? mb->pu[k] : (hand_on ? mb->pu[3] : nullptr);
+  R *nh = k < 3 ? mb->ph[k] : (hand_on ? mb->ph[3] : nullptr);
   RK<R, double> rut{du, nullptr, k == 3 ? du : nullptr, nu, c[k], w[k], R(0), ph.tc1};
   RK<R, double> rht{dh, nullptr, k == 3 ? dh : nullptr, nh, c[k], w[k], R(0), 0};
   if (k < 3) {
     rut.t_out = mb->tk_u[k];
     rht.t_out = mb->tk_h[k];
+    if (hand_on) {
+      rut.x0r = mb->pu[3];
+      rht.x0r = mb->ph[3];
+    }
   } else {
     for (int j = 0; j < 3; j++) {
       rut.t_in[j] = mb->tk_u[j];
@@ -554,11 +580,12 @@ static void tl_member_stage(Engine &E, int prec, int B, double *du, double *dh, 
     Launch<R, double>::tl_fused(E.fused, M, m, B, bs, uti, hti, ph, rut, rht, st);
     return;
   }
-  Launch<R, double>::tl_vertex(m, B, bs, uti, hti, mb->d, st);
-  Launch<R, double>::tl_cell(m, B, bs, uti, hti, mb->d, rht, nullptr, st);
-  Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, mb->d, ph, st);
-  if (ph.visc4 > R(0)) Launch<R, double>::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, st);
-  Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, mb->d, ph, rut, nullptr, st);
+  const Diag<R> d = tl_rows(mb, ph);
+  Launch<R, double>::tl_vertex(m, B, bs, uti, hti, d, st);
+  Launch<R, double>::tl_cell(m, B, bs, uti, hti, d, rht, nullptr, st);
+  Launch<R, double>::tl_edge_diag(m, B, bs, uti, hti, d, ph, st);
+  if (ph.visc4 > R(0)) Launch<R, double>::del4_vc(m, B, d.dsq_u, d.dsq_vort, d.dsq_div, st);
+  Launch<R, double>::tl_edge_tend(m, B, bs, uti, hti, d, ph, rut, nullptr, st);
 }
 
 // Copy B members' FP64 states between a caller's buffers and the engine's (internal order).
@@ -653,6 +680,10 @@ static void ad_member_step(Engine &E, int prec, int B, double *au, double *ah, M
     }
     out.x2u = au; out.x2h = ah; out.dst_u = au; out.dst_h = ah;
     out.mode = k == 3 ? AD_SET : k == 0 ? AD_FINAL : AD_ADD;
+    if (sizeof(R) == 4 && !ph.tc1) {  // the adjoint state rounded once per step (ad_tinit / AD_FINAL)
+      out.x2r_u = mb->pu[3];
+      out.x2r_h = mb->ph[3];
+    }
     out.tu_next = mb->pad_u[(4 - k) & 1];
     out.th_next = mb->pad_h[(4 - k) & 1];
     if (k > 0) {
@@ -667,7 +698,7 @@ static void ad_member_step(Engine &E, int prec, int B, double *au, double *ah, M
     if (const int M = fused_members<R>(E, B, ph))
       Launch<R, double>::ad_fused(E.fused, M, m, B, base(k), ph, in, out, E.stream);
     else
-      Launch<R, double>::ad_stage(m, B, base(k), ph, in, none, mb->w, out, E.stream);
+      Launch<R, double>::ad_stage(m, B, base(k), ph, in, none, ad_rows(mb, ph), out, E.stream);
   }
 }
 
@@ -688,6 +719,12 @@ static void window_ad_impl(Engine &E, int prec, int B, double *user_u, double *u
   // final stage of the step after them
   auto tinit = [&]() {
     Launch<R, double>::ad_tinit(m, B, au, ah, nullptr, nullptr, wu4, w[3], mb->pad_u[0], mb->pad_h[0], E.stream);
+    if constexpr (sizeof(R) == 4) {
+      if (!ph64.tc1) {  // the rounded adjoint state of the last step's stages
+        convert_d2f((long long)E.nE * B, au, mb->pu[3], E.stream);
+        convert_d2f((long long)E.nC * B, ah, mb->ph[3], E.stream);
+      }
+    }
   };
   if (W.st[prec].valid >= W.nsteps) {
     // stored linearisation points: the whole sweep is one graph of member kernels
@@ -882,6 +919,10 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters,
   RK<R, double> rkh{W.ms[prec].acc_h, nullptr, nullptr, mb->ph[1], c[1], w[1], R(0), 0};
   rku.t_out = mb->tk_u[1];
   rkh.t_out = mb->tk_h[1];
+  if (sizeof(R) == 4) {  // FP32 members read the step's rounded input
+    rku.x0r = mb->pu[3];
+    rkh.x0r = mb->ph[3];
+  }
   AdIn<R> in{mb->pad_u[0], mb->pad_h[0]};
   AdOut<R, double> out{};
   out.acc_u = W.ms[prec].acc_u; out.acc_h = W.ms[prec].acc_h; out.mode = AD_ADD;
@@ -889,34 +930,40 @@ static double time_kernel_impl(Engine &E, int which, int prec, int B, int iters,
   out.tu_next = mb->pad_u[1]; out.th_next = mb->pad_h[1];
   out.pad_out_u = mb->tk_u[1]; out.pad_out_h = mb->tk_h[1];
   out.wu = w[1]; out.cu = c[1]; out.wh = w[1]; out.ch = c[1];
+  if (sizeof(R) == 4) {
+    out.x2r_u = mb->pu[3];
+    out.x2r_h = mb->ph[3];
+  }
   StableBaseScope stable(true);  // the timed kernels write no linearisation point
+  const Diag<R> d = tl_rows(mb, ph);
+  const AdWork<R> aw = ad_rows(mb, ph);
   auto launch = [&]() {
     using LR = Launch<R, double>;
     switch (which) {
-      case 0: LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], mb->d, E.stream); break;
-      case 1: LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream); break;
-      case 2: LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream); break;
-      case 3: LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream); break;
+      case 0: LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], d, E.stream); break;
+      case 1: LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], d, rkh, nullptr, E.stream); break;
+      case 2: LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], d, ph, E.stream); break;
+      case 3: LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], d, ph, rku, nullptr, E.stream); break;
       case 8:  // one whole tangent-linear stage, as the sweeps run it
         if (const int M = fused_members<R>(E, B, ph)) {
           LR::tl_fused(E.fused, M, m, B, bs, mb->pu[0], mb->ph[0], ph, rku, rkh, E.stream);
           break;
         }
-        LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], mb->d, E.stream);
-        LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], mb->d, rkh, nullptr, E.stream);
-        LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, E.stream);
-        if (ph.visc4 > R(0)) LR::del4_vc(m, B, mb->d.dsq_u, mb->d.dsq_vort, mb->d.dsq_div, E.stream);
-        LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], mb->d, ph, rku, nullptr, E.stream);
+        LR::tl_vertex(m, B, bs, mb->pu[0], mb->ph[0], d, E.stream);
+        LR::tl_cell(m, B, bs, mb->pu[0], mb->ph[0], d, rkh, nullptr, E.stream);
+        LR::tl_edge_diag(m, B, bs, mb->pu[0], mb->ph[0], d, ph, E.stream);
+        if (ph.visc4 > R(0)) LR::del4_vc(m, B, d.dsq_u, d.dsq_vort, d.dsq_div, E.stream);
+        LR::tl_edge_tend(m, B, bs, mb->pu[0], mb->ph[0], d, ph, rku, nullptr, E.stream);
         break;
       case 9: {  // one whole adjoint stage, as the sweeps run it
         const AdSeeds<R> none{};
         if (const int M = fused_members<R>(E, B, ph))
           LR::ad_fused(E.fused, M, m, B, bs, ph, in, out, E.stream);
         else
-          LR::ad_stage(m, B, bs, ph, in, none, mb->w, out, E.stream);
+          LR::ad_stage(m, B, bs, ph, in, none, aw, out, E.stream);
         break;
       }
-      default: LR::ad_part(which - 4, m, B, bs, ph, in, mb->w, out, E.stream); break;
+      default: LR::ad_part(which - 4, m, B, bs, ph, in, aw, out, E.stream); break;
     }
   };
   launch();  // warm-up
