@@ -5,9 +5,10 @@ vertices), seeded balanced flow (seed 0) over 8 seeded mountains (h reduced by t
 dt = 75 s, a 288-step (6 h) window, trajectory checkpointed every 16 steps, perturbations
 h' ~ N(0, 1 m), u' ~ N(0, 0.1 m/s), B = 64 members.  One bench step is one gradient batch:
 the nonlinear window with checkpoints, the B-member tangent-linear sweep and the B-member
-adjoint sweep (seeded with the tangent-linear output, i.e. the gradient of 1/2 |L dx|^2).  `value` counts gradients of the batched FP32-stencil / FP64-accumulation
-form; the plain FP64 single-member form is timed beside it, with the relative L2 error of the
-batched result against the FP64 window.
+adjoint sweep (seeded with the tangent-linear output, i.e. the gradient of 1/2 |L dx|^2).
+`value` counts gradients of the batched FP32-stencil / FP64-accumulation form; the plain FP64
+single-member form is timed beside it, with the relative L2 error of the batched result against
+the FP64 window.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--batch B]
                   [--level L] [--nsteps T]
@@ -342,9 +343,10 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
     s: bytes of a member value, a linearisation-point value and a mesh metric (4 in FP32);
     accumulators and member RK states are a = 8 bytes; connectivity words 4 bytes, edge signs
     1 byte.  E, C, V: edges, cells, vertices.  RK bookkeeping of a middle stage, as the sweeps
-    and mpsw_time_kernel run it, reads the FP64 state x0 and writes the next provisional state
-    and the stage's tendency (a + 2s per member value); ad_final reads x2 and writes the next
-    tendency adjoint and its stage contribution (a + 2s)."""
+    and mpsw_time_kernel run it, reads the step's input state (FP32 members: its rounding, s
+    bytes; FP64: x0 itself) and writes the next provisional state and the stage's tendency
+    (3 s per member value); ad_final likewise reads x2 (rounded for FP32 members) and writes the
+    next tendency adjoint and its stage contribution (3 s)."""
     a, i, E, C, V, S = 8, 4, nE, nC, nV, sum_eoe
     eoe = i * (E + S) + s * S                              # nEdgesOnEdge, edgesOnEdge, weights
     kb = {
@@ -353,13 +355,13 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
                      + B * s * (E + C + V),                               # u,h in; pv out
         'tl_cell': (i + 3 * 6 * i + 6 + 6 * s + s) * C + (2 * i + 2 * s) * E  # c_n,es,eoc,vs,esg,kites,area; c1,c2,dc,dv
                    + 2 * s * E                                                  # base u, h_edge
-                   + B * (s * (E + C + V + 2 * C) + (a + 2 * s) * C),          # u,h,pv in; ke,pc out; RK
+                   + B * (s * (E + C + V + 2 * C) + 3 * s * C),                # u,h,pv in; ke,pc out; RK
         'tl_edge_diag': eoe + (6 * i + 2 * s) * E + 4 * s * E                  # ends; dc,dv; base gradPVt,v,gradPVn,u
                         + (2 * s * E if s == 4 else 0)                         # FP32: base h_edge, pv_edge
                         + B * s * (E + C + V + C + 2 * E)                      # u,h,pv,pc in; pv_edge,h_edge out
                         + (B * s * E if s == 4 else 0),                        # FP32: h_edge -> u h_edge, + PV flux
         'tl_edge_tend': eoe + (2 * i + s) * E + 3 * s * E                      # c1,c2,dc; base pv_edge,u,h_edge
-                        + B * (s * (3 * E + 2 * C) + (a + 2 * s) * E),         # u,pe,he,ke,h in; RK
+                        + B * (s * (3 * E + 2 * C) + 3 * s * E),               # u,pe,he,ke,h in; RK
         'ad_edge': eoe + s * S + (2 * i + s) * E + 6 * s * E                   # wrev; c1,c2,dv; 6 base fields
                    + B * s * (E + C + 3 * E),                                  # tu,th in; pe_ad,he_ad,ud out
         'ad_cell': (i + 6 * i + 6 + s) * C + 2 * s * E                         # c_n,es,esg,area; dc; base u
@@ -367,7 +369,7 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
         'ad_vertex': (3 * i + 3 * s + 3 * i + 3 * i + 3 + 2 * s) * V + s * C + 2 * s * E + 2 * s * V
                      + B * s * (C + E + 2 * V),                                # pc_ad,pe_ad in; 2 out
         'ad_final': (i + 6 * i + 6 * s + s) * C + i * (E + S) + s * S + (4 * i + 2 * s) * E + 2 * s * E
-                    + B * (s * (C + 2 * V + 2 * E + C) + (a + 2 * s) * (C + E)),
+                    + B * (s * (C + 2 * V + 2 * E + C) + 3 * s * (C + E)),
     }
     kb['tl_stage'] = sum(kb[k] for k in ('tl_vertex', 'tl_cell', 'tl_edge_diag', 'tl_edge_tend'))
     kb['ad_stage'] = sum(kb[k] for k in ('ad_edge', 'ad_cell', 'ad_vertex', 'ad_final'))
@@ -377,16 +379,17 @@ def kernel_bytes(name, nC, nE, nV, sum_eoe, B, s):
 def fused_bytes(name, nC, nE, nV, B, s=4, a=8):
     """Bytes a fused stage launch must move (a middle stage as the sweeps and mpsw_time_kernel run
     it; default physics): every mesh coefficient, linearisation-point value and member value it
-    touches, once.  Members: the stage's inputs (s), and the RK bookkeeping, which reads the FP64
-    state (a) and writes the next provisional state and the stage's tendency (tangent linear) or
-    its contribution and the next tendency adjoint (adjoint) (2 s): (3 s + a) per member value.
+    touches, once.  Members: the stage's inputs (s), and the RK bookkeeping, which reads the
+    step's rounded input state (s) and writes the next provisional state and the stage's tendency
+    (tangent linear) or its contribution and the next tendency adjoint (adjoint) (2 s): 4 s per
+    member value.
     Mesh, tangent linear: vertex 3+3 coefficients and f, cell 3 x 6 coefficients, edge 10 weights
     and two reciprocals; adjoint: both weight lists, dvEdge, dcEdge, cell 3 x 6 coefficients and
     areaCell, vertex 2 x 3 coefficients, areaTriangle and f.  Base: 6 edge and 2 vertex fields."""
     E, C, V = nE, nC, nV
     mesh = s * (7 * V + 18 * C + 12 * E) if name == 'tl_stage' else s * (22 * E + 19 * C + 8 * V)
     base = s * (6 * E + 2 * V)
-    return mesh + base + B * (E + C) * (3 * s + a)
+    return mesh + base + B * (E + C) * 4 * s
 
 
 def survey_stage_bytes(nC, nE, nV, sum_eoe, B, s=4, a=8):

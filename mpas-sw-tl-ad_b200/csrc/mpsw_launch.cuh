@@ -237,7 +237,7 @@ void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const 
                            const Diag<R> &d, const RK<R, A> &rk, R *tend_h, cudaStream_t s) {
   g_launches++;
   const int v = vec_width<R, A>(B, {ut, ht, d.div, d.ke, d.pc, d.vc, d.pvv, d.vort, tend_h, rk.x0, rk.acc_in,
-                                    rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1], rk.t_in[2]},
+                                    rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1], rk.t_in[2], rk.x0r},
                                 tuned_v(K_TL_CELL));
   const int bk = tuned_block(K_TL_CELL);
   if (use_staged(m, B, v, cell_stage_bytes<R>(), bk)) {
@@ -273,7 +273,7 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
   if (sizeof(R) == 4 && !d.v) throw std::invalid_argument("FP32 tl_edge_tend needs the PV-flux rows in d.v");
   const int v = vec_width<R, A>(B, {ut, ht, d.pe, d.he, d.v, d.ke, d.div, d.vort, d.dsq_div, d.dsq_vort, tend_u,
                                     rk.x0, rk.acc_in, rk.acc_out, rk.next, rk.t_out, rk.t_in[0], rk.t_in[1],
-                                    rk.t_in[2]},
+                                    rk.t_in[2], rk.x0r},
                                 tuned_v(K_TL_EDGE_TEND));
   const int bk = tuned_block(K_TL_EDGE_TEND);
   constexpr int J = BoundsNarrow::e2;
@@ -292,7 +292,7 @@ static int ad_width(int B, const AdIn<R> &in, const AdWork<R> &w, const AdOut<R,
                              w.ke_ad, w.div_ad, w.hd, w.dd_ad, w.hv_ad, w.circ_ad, w.dc_ad, out.acc_u, out.acc_h,
                              out.x2u, out.x2h, out.dst_u, out.dst_h, out.tu_next, out.th_next, out.pad_out_u,
                              out.pad_out_h, out.pad_in_u[0], out.pad_in_u[1], out.pad_in_u[2], out.pad_in_h[0],
-                             out.pad_in_h[1], out.pad_in_h[2]},
+                             out.pad_in_h[1], out.pad_in_h[2], out.x2r_u, out.x2r_h},
                          prefer);
 }
 
