@@ -130,8 +130,8 @@ def test_window_adjoint_vs_oracle_level5():
 
 @pytest.mark.parametrize('level,dt,nsteps', [(5, 300.0, 288), (6, 150.0, 96)])
 def test_fp32_window_within_bar(level, dt, nsteps):
-    """Batched FP32-stencil / FP64-accumulation TL and AD windows (64 members, the fused stage
-    kernels) within 1e-4 relative L2 of the FP64 window, member by member."""
+    """Batched FP32-stencil / FP64-accumulation TL and AD windows (64 members, the member kernels
+    the sweeps run by default) within 1e-4 relative L2 of the FP64 window, member by member."""
     from mpsw.torch_api import FP32, FP64, Engine
     g = setup(MpasSwModule(), level, 'seeded', dt=dt)
     e = Engine(g)
