@@ -21,8 +21,9 @@ def test_kernel_bytes_model():
     S = 10 * nE - 60
     fp32 = {k: bench.kernel_bytes(k, nC, nE, nV, S, 64, 4) for k in ('tl_stage', 'ad_stage', 'tl_edge_tend')}
     fp64 = {k: bench.kernel_bytes(k, nC, nE, nV, S, 64, 8) for k in ('tl_stage', 'ad_stage', 'tl_edge_tend')}
-    # the level-5, 64-member figures the bench line reports
-    assert fp32['tl_edge_tend'] == 63611424
+    # the level-5, 64-member figure: 3 E-rows gathered + 2 cell rows + the RK bookkeeping of a
+    # middle stage (rounded input read, provisional state and tendency written) + lists and base
+    assert fp32['tl_edge_tend'] == 55747104
     assert all(fp64[k] > fp32[k] for k in fp32)
     # members dominate: doubling B nearly doubles a stage's bytes
     assert 1.9 < bench.kernel_bytes('ad_stage', nC, nE, nV, S, 128, 4) / fp32['ad_stage'] < 2.0
