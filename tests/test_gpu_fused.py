@@ -101,9 +101,12 @@ def test_fused_members_per_chunk_and_block_size(nt):
     assert relmax(res[0], res[2]) < 1e-6
 
 
-def test_split_kernels_serve_other_physics():
-    """With viscosity, drag and wind the window runs the split kernels whatever MPSW_FUSED says."""
+def test_split_kernels_serve_other_physics(tmp_path, monkeypatch):
+    """With viscosity, drag and wind the window runs the split kernels whatever MPSW_FUSED says.
+    Both engines take their launch choices from one tuning cache: FP32 contraction may differ
+    between member widths, so the comparison is bit for bit only with the same choices."""
     from mpsw.torch_api import FP32
+    monkeypatch.setenv('MPSW_TUNE_CACHE', str(tmp_path / 'tune.txt'))
     B = 8
     cfg = dict(visc2=1e5, visc4=5e14, drag=True, wind=True)
     mf, ef = engine(4, {'MPSW_FUSED': '1'}, **cfg)
