@@ -41,7 +41,9 @@ def test_persistent_forward_matches_step_graphs(phys, precision):
 
 
 def test_persistent_forward_zero_steps_leaves_state():
+    """No step: time level 1 keeps the state (and time level 2 receives it, as after sw_rk4)."""
     g = setup(MpasSwModule(), 3, 'seeded')
-    u0, h0 = g.u.copy(), g.h.copy()
+    u0, h0 = g.u[0].copy(), g.h[0].copy()
     g.sw_rk4_steps(0, 1)
-    assert np.array_equal(g.u, u0) and np.array_equal(g.h, h0)
+    assert np.array_equal(g.u[0], u0) and np.array_equal(g.h[0], h0)
+    assert np.array_equal(g.u[1], u0) and np.array_equal(g.h[1], h0)
