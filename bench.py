@@ -795,10 +795,7 @@ def run_forward(a, rank, world):
             'rel_err_fp32_vs_fp64': err,
             'e2e': {'value': e2e, 'unit': 'sim-days/s', 'h2d_bytes_per_step': int((nC + nE) * 8),
                     'd2h_bytes_per_step': int((nC + nE) * 8)},
-            'roofline': {'bound': 'hbm',
-                         'kernel': ('k_fwd_persistent: the %d steps in one cooperative launch, 17 grid-barrier '
-                                    'phases a step' % a.nsteps) if launches < a.nsteps else 'one RK4 step (20 launches)',
-                         'achieved': ach, 'peak': hbm,
+            'roofline': {'bound': 'hbm', 'kernel': 'one RK4 step (20 launches)', 'achieved': ach, 'peak': hbm,
                          'unit': 'GB/s', 'frac': ach / hbm, 'traffic': None, 'algorithmic_bytes': bytes_step,
                          'peak_source': 'measured' if peaks.get('hbm_gbs') else 'fallback'},
             'cpu_baseline': cpu,

@@ -197,9 +197,8 @@ void Engine::need_device() {
   cuda_check(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate");
   for (cudaEvent_t *ev : {&ev_fork, &ev_step, &ev_join})
     cuda_check(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "cudaEventCreate");
-  // word 0: the non-finite flag; words 1-3: grid-barrier state of the persistent forward
-  cuda_check(cudaMalloc(&d_bad, 4 * sizeof(int)), "cudaMalloc flag");
-  cuda_check(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), stream), "clear flag");
+  cuda_check(cudaMalloc(&d_bad, sizeof(int)), "cudaMalloc flag");
+  cuda_check(cudaMemsetAsync(d_bad, 0, sizeof(int), stream), "clear flag");
 }
 
 Engine::~Engine() {
@@ -628,16 +627,13 @@ Phys<double> Engine::phys() const {
 // The flag the tendency kernels raise on a non-finite value: cleared at the start of a routine
 // (prepare, or a window sweep), read when it has finished.
 void Engine::nonfinite_clear() {
-  if (d_bad) cuda_check(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), stream), "clear non-finite flag");
+  if (d_bad) cuda_check(cudaMemsetAsync(d_bad, 0, sizeof(int), stream), "clear non-finite flag");
 }
 void Engine::nonfinite_check(const char *what) {
   if (!d_bad) return;
-  int w[4] = {0, 0, 0, 0};
-  cuda_check(cudaMemcpyAsync(w, d_bad, sizeof(w), cudaMemcpyDeviceToHost, stream), "read non-finite flag");
+  int v = 0;
+  cuda_check(cudaMemcpyAsync(&v, d_bad, sizeof(int), cudaMemcpyDeviceToHost, stream), "read non-finite flag");
   cuda_check(cudaStreamSynchronize(stream), what);
-  if (w[3])
-    throw EngineError(MPSW_ERR_CUDA, std::string(what) + ": a grid barrier of the persistent forward kernel timed out");
-  const int v = w[0];
   if (v)
     throw EngineError(MPSW_ERR_NONFINITE, std::string(what) +
                                               ": a tendency became non-finite (NaN or Inf); the state or the "
@@ -849,29 +845,13 @@ void Engine::rk4(int nsteps) {  // src/mpas_sw_module.f90:528-635
                           stream);
     }
   };
-  // without tracer transport one cooperative kernel for all the steps where it applies (the
-  // same per-entity arithmetic), else one CUDA graph per step (its buffers are fixed), captured
-  // on the first step
-  FwdPlan<double, double> plan{};
-  for (int k = 0; k < 4; k++) {
-    plan.ui[k] = k == 0 ? u0 : sp_u[k - 1];
-    plan.hi[k] = k == 0 ? h0 : sp_h[k - 1];
-    plan.ru[k] = RK<double, double>{u0, k == 0 ? u0 : acc_u, k == 3 ? u0 : acc_u, k < 3 ? sp_u[k] : nullptr,
-                                    c[k], w[k], 0.0, ph.tc1};
-    plan.rh[k] = RK<double, double>{h0, k == 0 ? h0 : acc_h, k == 3 ? h0 : acc_h, k < 3 ? sp_h[k] : nullptr,
-                                    c[k], w[k], 0.0, 0};
+  // one CUDA graph per step (its buffers are fixed), captured on the first step
+  GraphKey key = graph_key(8, 0, 1, u0, h0);
+  if (adv) {
+    key.p3 = tr0;
+    key.n2 = nT;
   }
-  plan.tu = dv("tend_u");
-  plan.th = dv("tend_h");
-  plan.bar = reinterpret_cast<unsigned *>(d_bad + 1);
-  if (adv || !L64::fwd_persistent(m64, d_cnb, 0.0, stage[0], ph, plan, nsteps, stream)) {
-    GraphKey key = graph_key(8, 0, 1, u0, h0);
-    if (adv) {
-      key.p3 = tr0;
-      key.n2 = nT;
-    }
-    for (int n = 0; n < nsteps; n++) run_graph(key, step);
-  }
+  for (int n = 0; n < nsteps; n++) run_graph(key, step);
   if (adv) tracers_download(tr0, trtend);
   finish_levels({"u", "h"});
   L64::recon(m64, 1, ph.sphere, u0, dv("uReconstructX"), dv("uReconstructY"), dv("uReconstructZ"),
@@ -931,27 +911,9 @@ void Engine::forward(int prec, int nsteps) {
       L32::fwd_edge_tend(m32, ui, hi, offf, d32, ph, ru, nullptr, stream);
     }
   };
-  // one cooperative kernel for all the steps where it applies, else one graph per step
-  FwdPlan<float, double> plan{};
-  for (int k = 0; k < 4; k++) {
-    plan.ui[k] = s32_u[k];
-    plan.hi[k] = s32_h[k];
-    plan.ru[k] = RK<float, double>{u0, k == 0 ? u0 : acc_u, k == 3 ? u0 : acc_u, k < 3 ? s32_u[k + 1] : nullptr,
-                                   c[k], w[k], 0.f, ph.tc1};
-    plan.rh[k] = RK<float, double>{h0, k == 0 ? h0 : acc_h, k == 3 ? h0 : acc_h, k < 3 ? s32_h[k + 1] : nullptr,
-                                   c[k], w[k], offf, 0};
-  }
-  plan.u0 = u0;
-  plan.h0 = h0;
-  plan.conv_u = s32_u[0];
-  plan.conv_h = s32_h[0];
-  plan.off = off;
-  plan.bar = reinterpret_cast<unsigned *>(d_bad + 1);
-  if (!L32::fwd_persistent(m32, d_cnb, offf, d32, ph, plan, nsteps, stream)) {
-    GraphKey key = graph_key(9, 1, 1, u0, h0);
-    std::memcpy(&key.n2, &off, sizeof(off));
-    for (int n = 0; n < nsteps; n++) run_graph(key, step);
-  }
+  GraphKey key = graph_key(9, 1, 1, u0, h0);
+  std::memcpy(&key.n2, &off, sizeof(off));
+  for (int n = 0; n < nsteps; n++) run_graph(key, step);
   finish_levels({"u", "h"});
   L64::recon(m64, 1, ph64.sphere, u0, dv("uReconstructX"), dv("uReconstructY"), dv("uReconstructZ"),
              dv("uReconstructZonal"), dv("uReconstructMeridional"), stream);

@@ -117,22 +117,6 @@ struct RK {
   const R *x0r;
 };
 
-// nsteps RK4 steps of one trajectory in one persistent kernel (k_fwd_persistent): stage k reads
-// ui[k], hi[k] and updates with ru[k], rh[k]; stage 4 also writes the tendencies tu, th (null:
-// not kept).  With conv_u set (reduced-precision stencils) each step first rounds the state u0
-// and h0 - off into conv_u, conv_h (= ui[0], hi[0]).  bar: three words of grid-barrier state
-// (arrivals, generation, error), zero at launch.
-template <typename R, typename A>
-struct FwdPlan {
-  const R *ui[4], *hi[4];
-  RK<R, A> ru[4], rh[4];
-  R *tu, *th;
-  const A *u0, *h0;
-  R *conv_u, *conv_h;
-  A off;
-  unsigned *bar;
-};
-
 // Input of one adjoint stage: its tendency adjoint, tu (edges) and th / areaCell (cells), as
 // formed by the previous adjoint stage (or k_ad_tinit) from src/mpas_sw_module.f90:912-942:
 // tend_ad = w * x2_ad + c * provis_ad(next stage) [+ seed].

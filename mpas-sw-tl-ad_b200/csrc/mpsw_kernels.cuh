@@ -43,24 +43,6 @@ __device__ __forceinline__ R ld(const R *p, size_t i) {
   return __ldg(p + i);
 }
 
-// Loads in the forward bodies, which run in their own kernels (P = false) or as phases of the
-// persistent forward kernel (P = true), whose blocks read after a grid barrier what other blocks
-// wrote before it: there every array the kernel writes (stage inputs, diagnostics, RK states) is
-// read through L2 (ld.global.cg), since L1 is not coherent across SMs and the read-only path
-// must not see data written during the kernel.
-// ldi: a stage input (read-only path in a kernel of its own); ldw: an array written by an
-// earlier kernel or phase (plain load in a kernel of its own).
-template <bool P, typename T>
-__device__ __forceinline__ T ldi(const T *p, size_t i) {
-  if constexpr (P) return __ldcg(p + i);
-  else return __ldg(p + i);
-}
-template <bool P, typename T>
-__device__ __forceinline__ T ldw(const T *p, size_t i) {
-  if constexpr (P) return __ldcg(p + i);
-  else return p[i];
-}
-
 // Bounds of the neighbour loops.  BoundsNarrow serves meshes with at most 10 edgesOnEdge and 6
 // edgesOnCell (every quasi-uniform hexagon/pentagon mesh): the loops get compile-time trip
 // counts and are unrolled with `slot < n` as a predicate, so the connectivity, weight and member
@@ -91,273 +73,195 @@ struct BoundsAny {
 // ----------------------------------------------------------------------------------------
 
 // circulation/vorticity (:208-219), h_vertex and pv_vertex (:282-292)
-template <typename R, bool P>
-__device__ __forceinline__ void fwd_vertex_at(const MeshDev<R> &m, const R *__restrict__ u, const R *__restrict__ h,
-                                              R off, const Diag<R> &d, int v) {
-  const int nV = m.nV;
-  R circ = R(0);
-#pragma unroll
-  for (int k = 0; k < VDEG; k++) {
-    const int e = ld(m.v_es, (size_t)k * nV + v);
-    const R s = R(m.v_esg[(size_t)k * nV + v]);
-    circ = circ + s * (ld(m.e_dc, e) * ldi<P>(u, e));
-  }
-  const R area = ld(m.v_area, v);
-  const R vort = circ / area;
-  R hv = R(0);
-#pragma unroll
-  for (int k = 0; k < VDEG; k++)
-    hv = hv + (ldi<P>(h, ld(m.v_c, (size_t)k * nV + v)) + off) * ld(m.v_k, (size_t)k * nV + v);
-  hv = hv / area;
-  const R pv = (ld(m.v_f, v) + vort) / hv;
-  if (d.circ) d.circ[v] = circ;
-  d.vort[v] = vort;
-  d.hv[v] = hv;
-  d.pvv[v] = pv;
-}
 template <typename R>
 __global__ void k_fwd_vertex(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ h, R off,
                              Diag<R> d) {
-  MPSW_GRID_LOOP(t, m.nV) fwd_vertex_at<R, false>(m, u, h, off, d, (int)t);
+  const int nV = m.nV;
+  MPSW_GRID_LOOP(t, nV) {
+    const int v = (int)t;
+    R circ = R(0);
+#pragma unroll
+    for (int k = 0; k < VDEG; k++) {
+      const int e = ld(m.v_es, (size_t)k * nV + v);
+      const R s = R(m.v_esg[(size_t)k * nV + v]);
+      circ = circ + s * (ld(m.e_dc, e) * ld(u, e));
+    }
+    const R area = ld(m.v_area, v);
+    const R vort = circ / area;
+    R hv = R(0);
+#pragma unroll
+    for (int k = 0; k < VDEG; k++)
+      hv = hv + (ld(h, ld(m.v_c, (size_t)k * nV + v)) + off) * ld(m.v_k, (size_t)k * nV + v);
+    hv = hv / area;
+    const R pv = (ld(m.v_f, v) + vort) / hv;
+    if (d.circ) d.circ[v] = circ;
+    d.vort[v] = vort;
+    d.hv[v] = hv;
+    d.pvv[v] = pv;
+  }
 }
 
 // divergence (:222-242), ke (:245-256), pv_cell/vorticity_cell (:324-340) and the thickness
 // tendency (:468-482) with its RK update.
 // c_nb[k][c] is the cell across edge k of the cell (its h_edge sums this cell's h and that
 // cell's, in either order: the same value)
-template <typename R, typename A, int NC, bool P>
-__device__ __forceinline__ void fwd_cell_at(const MeshDev<R> &m, const int *__restrict__ c_nb,
-                                            const R *__restrict__ u, const R *__restrict__ h, R off,
-                                            const Diag<R> &d, const RK<R, A> &rk, R *tend_h, int c) {
-  const int nC = m.nC;
-  const int n = ld(m.c_n, c);
-  const R hc = ldi<P>(h, c) + off;
-  R div = R(0), th = R(0);
-  MPSW_PADDED(k, NC, n) {
-    const int e = ld(m.c_es, (size_t)k * nC + c);
-    const R s = R(m.c_esg[(size_t)k * nC + c]);
-    const R ue = ldi<P>(u, e), dve = ld(m.e_dv, e);
-    div = div + s * (ue * dve);
-    const R he = R(0.5) * (hc + (ldi<P>(h, ld(c_nb, (size_t)k * nC + c)) + off));
-    th = th + (-s) * ((ue * dve) * he);
-  }
-  const R area = ld(m.c_area, c);
-  div = div * (R(1) / area);
-  R ke = R(0);
-  for (int i = 0; i < n; i++) {
-    const int e = ld(m.c_eoc, (size_t)i * nC + c);
-    const R ue = ldi<P>(u, e);
-    ke = ke + ((R(0.25) * ld(m.e_dc, e)) * ld(m.e_dv, e)) * (ue * ue);
-  }
-  R pc = R(0), vc = R(0);
-  if constexpr (sizeof(R) == 4) {
-    // FP32 stencils: 1 / areaCell formed once instead of eight divisions
-    const R ra = R(1) / area;
-    ke = ke * ra;
-    MPSW_PADDED(k, NC, n) {
-      const int v = ld(m.c_vs, (size_t)k * nC + c);
-      const R kr = ld(m.c_vk, (size_t)k * nC + c) * ra;
-      pc = pc + kr * ldw<P>(d.pvv, v);
-      if (d.vc) vc = vc + kr * ldw<P>(d.vort, v);
-    }
-    th = th * ra;
-  } else {
-    ke = ke / area;
-    MPSW_PADDED(k, NC, n) {
-      const int v = ld(m.c_vs, (size_t)k * nC + c);
-      const R kt = ld(m.c_vk, (size_t)k * nC + c);
-      pc = pc + (kt * ldw<P>(d.pvv, v)) / area;
-      if (d.vc) vc = vc + (kt * ldw<P>(d.vort, v)) / area;
-    }
-    th = th / area;
-  }
-  d.div[c] = div;
-  d.ke[c] = ke;
-  d.pc[c] = pc;
-  if (d.vc) d.vc[c] = vc;
-  if (tend_h) tend_h[c] = th;
-  if (rk.next) rk.next[c] = R((ldw<P>(rk.x0, c) - A(rk.off)) + rk.c * A(th));
-  if (rk.acc_out) rk.acc_out[c] = ldw<P>(rk.acc_in, c) + rk.w * A(th);
-}
 template <typename R, typename A, int NC>
 __global__ void k_fwd_cell(MeshDev<R> m, const int *__restrict__ c_nb, const R *__restrict__ u,
                            const R *__restrict__ h, R off, Diag<R> d, RK<R, A> rk, R *tend_h) {
-  MPSW_GRID_LOOP(t, m.nC) fwd_cell_at<R, A, NC, false>(m, c_nb, u, h, off, d, rk, tend_h, (int)t);
+  const int nC = m.nC;
+  MPSW_GRID_LOOP(t, nC) {
+    const int c = (int)t;
+    const int n = ld(m.c_n, c);
+    const R hc = ld(h, c) + off;
+    R div = R(0), th = R(0);
+    MPSW_PADDED(k, NC, n) {
+      const int e = ld(m.c_es, (size_t)k * nC + c);
+      const R s = R(m.c_esg[(size_t)k * nC + c]);
+      const R ue = ld(u, e), dve = ld(m.e_dv, e);
+      div = div + s * (ue * dve);
+      const R he = R(0.5) * (hc + (ld(h, ld(c_nb, (size_t)k * nC + c)) + off));
+      th = th + (-s) * ((ue * dve) * he);
+    }
+    const R area = ld(m.c_area, c);
+    div = div * (R(1) / area);
+    R ke = R(0);
+    for (int i = 0; i < n; i++) {
+      const int e = ld(m.c_eoc, (size_t)i * nC + c);
+      const R ue = ld(u, e);
+      ke = ke + ((R(0.25) * ld(m.e_dc, e)) * ld(m.e_dv, e)) * (ue * ue);
+    }
+    R pc = R(0), vc = R(0);
+    if constexpr (sizeof(R) == 4) {
+      // FP32 stencils: 1 / areaCell formed once instead of eight divisions
+      const R ra = R(1) / area;
+      ke = ke * ra;
+      MPSW_PADDED(k, NC, n) {
+        const int v = ld(m.c_vs, (size_t)k * nC + c);
+        const R kr = ld(m.c_vk, (size_t)k * nC + c) * ra;
+        pc = pc + kr * d.pvv[v];
+        if (d.vc) vc = vc + kr * d.vort[v];
+      }
+      th = th * ra;
+    } else {
+      ke = ke / area;
+      MPSW_PADDED(k, NC, n) {
+        const int v = ld(m.c_vs, (size_t)k * nC + c);
+        const R kt = ld(m.c_vk, (size_t)k * nC + c);
+        pc = pc + (kt * d.pvv[v]) / area;
+        if (d.vc) vc = vc + (kt * d.vort[v]) / area;
+      }
+      th = th / area;
+    }
+    d.div[c] = div;
+    d.ke[c] = ke;
+    d.pc[c] = pc;
+    if (d.vc) d.vc[c] = vc;
+    if (tend_h) tend_h[c] = th;
+    if (rk.next) rk.next[c] = R((rk.x0[c] - A(rk.off)) + rk.c * A(th));
+    if (rk.acc_out) rk.acc_out[c] = rk.acc_in[c] + rk.w * A(th);
+  }
 }
 
 // tangential velocity (:259-267), gradPVt (:296-301), pv_edge with both APVM terms
 // (:305-320, :344-359), h_edge (:95-105) and, for del4, delsq_u (:539-551).
-template <typename R, int NE, bool P>
-__device__ __forceinline__ void fwd_edge_diag_at(const MeshDev<R> &m, const R *__restrict__ u,
-                                                 const R *__restrict__ h, R off, const Diag<R> &d,
-                                                 const Phys<R> &ph, int e) {
-  const int nE = m.nE;
-  const int n = ld(m.e_n, e);
-  R v = R(0);
-  MPSW_PADDED(j, NE, n)
-    v = v + ld(m.e_w, (size_t)j * nE + e) * ldi<P>(u, ld(m.e_eoe, (size_t)j * nE + e));
-  const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
-  const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
-  const R pv1 = ldw<P>(d.pvv, v1), pv2 = ldw<P>(d.pvv, v2);
-  const R gpt = (pv2 - pv1) / dv;
-  // pv_edge's two vertex terms: the reference adds them over edgesOnVertex, which lists the
-  // same two endpoints; a sum of two terms is the same in either order
-  R pe = R(0);
-  pe = pe + R(0.5) * pv1;
-  pe = pe + R(0.5) * pv2;
-  pe = pe - ((ph.apvm * v) * ph.dt) * gpt;
-  const R gpn = (ldw<P>(d.pc, c2) - ldw<P>(d.pc, c1)) / dc;
-  pe = pe - ((ph.apvm * ldi<P>(u, e)) * ph.dt) * gpn;
-  d.pe[e] = pe;
-  const R he = R(0.5) * ((ldi<P>(h, c1) + off) + (ldi<P>(h, c2) + off));
-  if constexpr (sizeof(R) == 4) {
-    // FP32 stencils: the edge's thickness flux u h_edge in d.he and PV flux u h_edge pv_edge
-    // in d.v, the two values k_fwd_edge_tend gathers at the neighbours
-    const R f = ldi<P>(u, e) * he;
-    d.he[e] = f;
-    d.v[e] = f * pe;
-  } else {
-    d.he[e] = he;
-    if (d.v) d.v[e] = v;
-  }
-  if (d.gpt) d.gpt[e] = gpt;
-  if (d.gpn) d.gpn[e] = gpn;
-  if (d.dsq_u)
-    d.dsq_u[e] = (ldw<P>(d.div, c2) - ldw<P>(d.div, c1)) / dc - (ldw<P>(d.vort, v2) - ldw<P>(d.vort, v1)) / dv;
-}
 template <typename R, int NE>
 __global__ void k_fwd_edge_diag(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ h, R off,
                                 Diag<R> d, Phys<R> ph) {
-  MPSW_GRID_LOOP(t, m.nE) fwd_edge_diag_at<R, NE, false>(m, u, h, off, d, ph, (int)t);
+  const int nE = m.nE;
+  MPSW_GRID_LOOP(t, nE) {
+    const int e = (int)t;
+    const int n = ld(m.e_n, e);
+    R v = R(0);
+    MPSW_PADDED(j, NE, n)
+      v = v + ld(m.e_w, (size_t)j * nE + e) * ld(u, ld(m.e_eoe, (size_t)j * nE + e));
+    const int v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e), c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e);
+    const R dv = ld(m.e_dv, e), dc = ld(m.e_dc, e);
+    const R pv1 = d.pvv[v1], pv2 = d.pvv[v2];
+    const R gpt = (pv2 - pv1) / dv;
+    // pv_edge's two vertex terms: the reference adds them over edgesOnVertex, which lists the
+    // same two endpoints; a sum of two terms is the same in either order
+    R pe = R(0);
+    pe = pe + R(0.5) * pv1;
+    pe = pe + R(0.5) * pv2;
+    pe = pe - ((ph.apvm * v) * ph.dt) * gpt;
+    const R gpn = (d.pc[c2] - d.pc[c1]) / dc;
+    pe = pe - ((ph.apvm * ld(u, e)) * ph.dt) * gpn;
+    d.pe[e] = pe;
+    const R he = R(0.5) * ((ld(h, c1) + off) + (ld(h, c2) + off));
+    if constexpr (sizeof(R) == 4) {
+      // FP32 stencils: the edge's thickness flux u h_edge in d.he and PV flux u h_edge pv_edge
+      // in d.v, the two values k_fwd_edge_tend gathers at the neighbours
+      const R f = ld(u, e) * he;
+      d.he[e] = f;
+      d.v[e] = f * pe;
+    } else {
+      d.he[e] = he;
+      if (d.v) d.v[e] = v;
+    }
+    if (d.gpt) d.gpt[e] = gpt;
+    if (d.gpn) d.gpn[e] = gpn;
+    if (d.dsq_u) d.dsq_u[e] = (d.div[c2] - d.div[c1]) / dc - (d.vort[v2] - d.vort[v1]) / dv;
+  }
 }
 
 // Normal-velocity tendency (src/mpas_sw_dyncore.f90:485-637) and its RK update.
-template <typename R, typename A, int NE, bool P>
-__device__ __forceinline__ void fwd_edge_tend_at(const MeshDev<R> &m, const R *__restrict__ u,
-                                                 const R *__restrict__ h, R off, const Diag<R> &d,
-                                                 const Phys<R> &ph, const RK<R, A> &rk, R *tend_u, int e) {
-  const int nE = m.nE;
-  const int n = ld(m.e_n, e);
-  const R pee = ldw<P>(d.pe, e);
-  R q = R(0);
-  if constexpr (sizeof(R) == 4) {
-    // FP32 stencils: q = 0.5 pv_edge(e) sum w (u h_edge)_j + 0.5 sum w (u h_edge pv_edge)_j,
-    // the same sum regrouped by the neighbour fluxes k_fwd_edge_diag leaves in d.he and d.v
-    R f1 = R(0), f2 = R(0);
-    MPSW_PADDED(j, NE, n) {
-      const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
-      const R w = ld(m.e_w, (size_t)j * nE + e);
-      f1 = f1 + w * ldw<P>(d.he, eoe);
-      f2 = f2 + w * ldw<P>(d.v, eoe);
-    }
-    q = (R(0.5) * pee) * f1 + R(0.5) * f2;
-  } else {
-    MPSW_PADDED(j, NE, n) {
-      const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
-      const R wpv = R(0.5) * (pee + ldw<P>(d.pe, eoe));
-      q = q + ((ld(m.e_w, (size_t)j * nE + e) * ldi<P>(u, eoe)) * wpv) * ldw<P>(d.he, eoe);
-    }
-  }
-  const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
-  const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
-  R grav;
-  if constexpr (std::is_same<R, double>::value) {
-    grav = R(GRAVITY) * ((((ldi<P>(h, c2) + off) + ld(m.c_hs, c2)) - (ldi<P>(h, c1) + off)) - ld(m.c_hs, c1));
-  } else {  // reduced precision: difference the offset-free values first
-    grav = R(GRAVITY) * ((ldi<P>(h, c2) - ldi<P>(h, c1)) + (ld(m.c_hs, c2) - ld(m.c_hs, c1)));
-  }
-  R tu = q - ((ldw<P>(d.ke, c2) - ldw<P>(d.ke, c1)) + grav) / dc;
-  if (ph.visc2 > R(0)) {
-    R ud = (ldw<P>(d.div, c2) - ldw<P>(d.div, c1)) / dc - (ldw<P>(d.vort, v2) - ldw<P>(d.vort, v1)) / dv;
-    ud = (ld(m.e_sc2, e) * ph.visc2) * ud;
-    tu = tu + ud;
-  }
-  if (ph.visc4 > R(0)) {
-    R ud = (ldw<P>(d.dsq_div, c2) - ldw<P>(d.dsq_div, c1)) / dc - (ldw<P>(d.dsq_vort, v2) - ldw<P>(d.dsq_vort, v1)) / dv;
-    ud = (ld(m.e_sc4, e) * ph.visc4) * ud;
-    tu = tu - ud;
-  }
-  // h_edge of the edge itself (d.he holds the thickness flux with FP32 stencils)
-  const R hee = sizeof(R) == 4 ? R(0.5) * ((ldi<P>(h, c1) + off) + (ldi<P>(h, c2) + off)) : ldw<P>(d.he, e);
-  if (ph.wind) tu = tu + (ld(m.e_usrc, e) / R(RHO_REF)) / hee;
-  if (ph.drag) {
-    const R kee = R(0.5) * (ldw<P>(d.ke, c1) + ldw<P>(d.ke, c2));
-    tu = tu - ((R(1.0e-3) * ldi<P>(u, e)) * sqrt(R(2) * kee)) / hee;
-  }
-  if (ph.bad && !isfinite(tu)) *ph.bad = 1;
-  if (tend_u) tend_u[e] = tu;
-  if (rk.next) rk.next[e] = rk.frozen ? R(ldw<P>(rk.x0, e)) : R(ldw<P>(rk.x0, e) + rk.c * A(tu));
-  if (rk.acc_out && !rk.frozen) rk.acc_out[e] = ldw<P>(rk.acc_in, e) + rk.w * A(tu);
-}
 template <typename R, typename A, int NE>
 __global__ void k_fwd_edge_tend(MeshDev<R> m, const R *__restrict__ u, const R *__restrict__ h, R off,
                                 Diag<R> d, Phys<R> ph, RK<R, A> rk, R *tend_u) {
-  MPSW_GRID_LOOP(t, m.nE) fwd_edge_tend_at<R, A, NE, false>(m, u, h, off, d, ph, rk, tend_u, (int)t);
-}
-
-// ---- persistent forward ------------------------------------------------------------------
-// Grid barrier of a cooperative launch (all blocks resident).  bar[0] counts arrivals, bar[1] is
-// the generation, bar[2] the error flag.  Thread 0 of each block arrives after a fence; the last
-// arrival resets the count and advances the generation, the others poll it.  A poll gives up
-// after kBarrierPolls (about a second), or as soon as another block has given up: it raises the
-// error flag and the block returns false, so every block leaves the kernel and no block waits
-// on one that has stopped.
-constexpr long long kBarrierPolls = 1LL << 21;
-__device__ __forceinline__ bool grid_barrier(unsigned *bar) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned *vb = bar;
-    ok = 1;
-    const unsigned g = vb[1];
-    __threadfence();
-    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
-      vb[0] = 0;
-      __threadfence();
-      atomicAdd(&bar[1], 1u);
+  const int nE = m.nE;
+  MPSW_GRID_LOOP(t, nE) {
+    const int e = (int)t;
+    const int n = ld(m.e_n, e);
+    const R pee = d.pe[e];
+    R q = R(0);
+    if constexpr (sizeof(R) == 4) {
+      // FP32 stencils: q = 0.5 pv_edge(e) sum w (u h_edge)_j + 0.5 sum w (u h_edge pv_edge)_j,
+      // the same sum regrouped by the neighbour fluxes k_fwd_edge_diag leaves in d.he and d.v
+      R f1 = R(0), f2 = R(0);
+      MPSW_PADDED(j, NE, n) {
+        const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
+        const R w = ld(m.e_w, (size_t)j * nE + e);
+        f1 = f1 + w * d.he[eoe];
+        f2 = f2 + w * d.v[eoe];
+      }
+      q = (R(0.5) * pee) * f1 + R(0.5) * f2;
     } else {
-      for (long long n = 0; vb[1] == g; n++) {
-        if (vb[2] || n > kBarrierPolls) {
-          atomicExch(&bar[2], 1u);
-          ok = 0;
-          break;
-        }
-        __nanosleep(100);
+      MPSW_PADDED(j, NE, n) {
+        const int eoe = ld(m.e_eoe, (size_t)j * nE + e);
+        const R wpv = R(0.5) * (pee + d.pe[eoe]);
+        q = q + ((ld(m.e_w, (size_t)j * nE + e) * ld(u, eoe)) * wpv) * d.he[eoe];
       }
     }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
-// nsteps RK4 steps in one kernel: the phases of each stage (vertex, cell, edge diagnostics, edge
-// tendency; the same per-entity bodies as the four forward kernels, with every array the kernel
-// writes read through L2) separated by grid barriers, which replace the 16-20 launches of a step
-// (default physics: no del4).  Launched cooperatively with every block resident.
-template <typename R, typename A, int NC, int NE>
-__global__ void __launch_bounds__(256) k_fwd_persistent(MeshDev<R> m, const int *__restrict__ c_nb, R off,
-                                                        Diag<R> d, Phys<R> ph, FwdPlan<R, A> p, int nsteps) {
-  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
-  for (int s = 0; s < nsteps; s++) {
-    if (p.conv_u) {
-      for (long long t = t0; t < m.nE; t += nt) p.conv_u[t] = R(__ldcg(p.u0 + t));
-      for (long long t = t0; t < m.nC; t += nt) p.conv_h[t] = R(__ldcg(p.h0 + t) - p.off);
-      if (!grid_barrier(p.bar)) return;
+    const int c1 = ld(m.e_c1, e), c2 = ld(m.e_c2, e), v1 = ld(m.e_v1, e), v2 = ld(m.e_v2, e);
+    const R dc = ld(m.e_dc, e), dv = ld(m.e_dv, e);
+    R grav;
+    if constexpr (std::is_same<R, double>::value) {
+      grav = R(GRAVITY) * ((((ld(h, c2) + off) + ld(m.c_hs, c2)) - (ld(h, c1) + off)) - ld(m.c_hs, c1));
+    } else {  // reduced precision: difference the offset-free values first
+      grav = R(GRAVITY) * ((ld(h, c2) - ld(h, c1)) + (ld(m.c_hs, c2) - ld(m.c_hs, c1)));
     }
-    for (int k = 0; k < 4; k++) {
-      const R *u = p.ui[k], *h = p.hi[k];
-      for (long long t = t0; t < m.nV; t += nt) fwd_vertex_at<R, true>(m, u, h, off, d, (int)t);
-      if (!grid_barrier(p.bar)) return;
-      for (long long t = t0; t < m.nC; t += nt)
-        fwd_cell_at<R, A, NC, true>(m, c_nb, u, h, off, d, p.rh[k], k == 3 ? p.th : nullptr, (int)t);
-      if (!grid_barrier(p.bar)) return;
-      for (long long t = t0; t < m.nE; t += nt) fwd_edge_diag_at<R, NE, true>(m, u, h, off, d, ph, (int)t);
-      if (!grid_barrier(p.bar)) return;
-      for (long long t = t0; t < m.nE; t += nt)
-        fwd_edge_tend_at<R, A, NE, true>(m, u, h, off, d, ph, p.ru[k], k == 3 ? p.tu : nullptr, (int)t);
-      if (!grid_barrier(p.bar)) return;
+    R tu = q - ((d.ke[c2] - d.ke[c1]) + grav) / dc;
+    if (ph.visc2 > R(0)) {
+      R ud = (d.div[c2] - d.div[c1]) / dc - (d.vort[v2] - d.vort[v1]) / dv;
+      ud = (ld(m.e_sc2, e) * ph.visc2) * ud;
+      tu = tu + ud;
     }
+    if (ph.visc4 > R(0)) {
+      R ud = (d.dsq_div[c2] - d.dsq_div[c1]) / dc - (d.dsq_vort[v2] - d.dsq_vort[v1]) / dv;
+      ud = (ld(m.e_sc4, e) * ph.visc4) * ud;
+      tu = tu - ud;
+    }
+    // h_edge of the edge itself (d.he holds the thickness flux with FP32 stencils)
+    const R hee = sizeof(R) == 4 ? R(0.5) * ((ld(h, c1) + off) + (ld(h, c2) + off)) : d.he[e];
+    if (ph.wind) tu = tu + (ld(m.e_usrc, e) / R(RHO_REF)) / hee;
+    if (ph.drag) {
+      const R kee = R(0.5) * (d.ke[c1] + d.ke[c2]);
+      tu = tu - ((R(1.0e-3) * ld(u, e)) * sqrt(R(2) * kee)) / hee;
+    }
+    if (ph.bad && !isfinite(tu)) *ph.bad = 1;
+    if (tend_u) tend_u[e] = tu;
+    if (rk.next) rk.next[e] = rk.frozen ? R(rk.x0[e]) : R(rk.x0[e] + rk.c * A(tu));
+    if (rk.acc_out && !rk.frozen) rk.acc_out[e] = rk.acc_in[e] + rk.w * A(tu);
   }
 }
 

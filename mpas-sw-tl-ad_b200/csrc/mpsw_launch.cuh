@@ -423,39 +423,6 @@ bool Launch<R, A>::fused_ok(const FusedDev &f, int B, const Phys<R> &ph, int M) 
     default: throw std::invalid_argument("fused stage: unsupported members per chunk or block size"); \
   }
 
-// Blocks per SM of the persistent forward: as many 256-thread blocks as fit (the gathers want
-// the occupancy), or MPSW_PERSIST_BPS when set lower.
-template <typename R, typename A>
-bool Launch<R, A>::fwd_persistent(const MeshDev<R> &m, const int *c_nb, R off, const Diag<R> &d, const Phys<R> &ph,
-                                  const FwdPlan<R, A> &p, int nsteps, cudaStream_t s) {
-  const char *on = std::getenv("MPSW_PERSIST");
-  if ((on && std::atoi(on) == 0) || ph.visc4 > R(0) || m.max_eoe > BoundsNarrow::e2 || m.max_eoc > BoundsNarrow::c)
-    return false;
-  auto kernel = k_fwd_persistent<R, A, BoundsNarrow::c, BoundsNarrow::e2>;
-  int dev = 0, sms = 0, per = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0) != cudaSuccess || per < 1)
-    return false;
-  const char *bps = std::getenv("MPSW_PERSIST_BPS");
-  if (bps && std::atoi(bps) > 0 && std::atoi(bps) < per) per = std::atoi(bps);
-  if (nsteps <= 0) return true;
-  g_launches++;
-  (void)cudaMemsetAsync(p.bar, 0, 3 * sizeof(unsigned), s);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(sms * per));
-  cfg.blockDim = dim3(256);
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeCooperative;
-  at[0].val.cooperative = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  // a failed launch is reported by the cudaGetLastError check that follows
-  (void)cudaLaunchKernelEx(&cfg, kernel, m, c_nb, off, d, ph, p, nsteps);
-  return true;
-}
-
 template <typename R, typename A>
 cudaError_t Launch<R, A>::fused_prepare(const FusedDev &f) {
   if constexpr (std::is_same<R, float>::value && std::is_same<A, double>::value) {

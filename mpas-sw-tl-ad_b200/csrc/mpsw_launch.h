@@ -89,11 +89,6 @@ struct Launch {
                        const AdIn<R> &in, const AdOut<R, A> &out, cudaStream_t s);
   // raise the fused kernels' dynamic shared-memory limit to what the tiles need
   static cudaError_t fused_prepare(const FusedDev &f);
-  // nsteps forward steps as one cooperative launch of k_fwd_persistent (p.bar cleared first);
-  // false, launching nothing, where it does not apply (del4 viscosity, meshes beyond 10
-  // edgesOnEdge or 6 edges per cell, MPSW_PERSIST=0, no resident block)
-  static bool fwd_persistent(const MeshDev<R> &m, const int *c_nb, R off, const Diag<R> &d, const Phys<R> &ph,
-                             const FwdPlan<R, A> &p, int nsteps, cudaStream_t s);
   static void ad_tinit(const MeshDev<R> &m, int B, const A *x2u, const A *x2h, const R *seed_tu,
                        const R *seed_th, A wu, A wh, R *tu, R *th, cudaStream_t s);
   static void recon_adj(const MeshDev<R> &m, int sphere, R *Xa, R *Ya, R *Za, R *Zoa, R *Mea, A *u_ad,
