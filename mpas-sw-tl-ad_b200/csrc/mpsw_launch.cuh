@@ -260,7 +260,7 @@ void Launch<R, A>::tl_edge_diag(const MeshDev<R> &m, int B, const Base<R> &bs, c
   constexpr int J = BoundsNarrow::e2;
   constexpr size_t eb = eoe_stage_bytes<R, J, 1, 0>();
   if (use_staged(m, B, v, eb, bk)) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_edge_diag_st<R, VV, J>, staged_cfg(m.nE, B, VV, eb, bk), s, m, B, bs, ut, ht, dd, ph, (int)g_stable_base));
+    MPSW_VDISPATCH(v, launch_k(tl_edge_diag_st_kernel<R, VV, J>(), staged_cfg(m.nE, B, VV, eb, bk), s, m, B, bs, ut, ht, dd, ph, (int)g_stable_base));
     return;
   }
   MPSW_VDISPATCH(v, MPSW_BDISPATCH(m, launch_k(k_tl_edge_diag<R, VV, NB>, launch_cfg((long long)(m.nE) * ((B) / (VV)), bk), s, m, B, bs, ut, ht, dd, ph)));
@@ -279,7 +279,7 @@ void Launch<R, A>::tl_edge_tend(const MeshDev<R> &m, int B, const Base<R> &bs, c
   constexpr int J = BoundsNarrow::e2;
   constexpr size_t eb = eoe_stage_bytes<R, J, 1, 3>();
   if (use_staged(m, B, v, eb, bk)) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_edge_tend_st<R, A, VV, J>, staged_cfg(m.nE, B, VV, eb, bk),
+    MPSW_VDISPATCH(v, launch_k(tl_edge_tend_st_kernel<R, A, VV, J>(), staged_cfg(m.nE, B, VV, eb, bk),
                                s, m, B, bs, ut, ht, d, ph, rk, tend_u, (int)g_stable_base));
     return;
   }
