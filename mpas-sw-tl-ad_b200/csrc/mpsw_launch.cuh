@@ -226,7 +226,7 @@ void Launch<R, A>::tl_vertex(const MeshDev<R> &m, int B, const Base<R> &bs, cons
   const int v = vec_width<R, A>(B, {ut, ht, d.circ, d.vort, d.hv, d.pvv}, tuned_v(K_TL_VERTEX));
   const int bk = tuned_block(K_TL_VERTEX);
   if (use_staged(m, B, v, vertex_stage_bytes<R>(), bk)) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_vertex_st<R, VV>, staged_cfg(m.nV, B, VV, vertex_stage_bytes<R>(), bk), s, m, B,
+    MPSW_VDISPATCH(v, launch_k(tl_vertex_st_kernel<R, VV>(), staged_cfg(m.nV, B, VV, vertex_stage_bytes<R>(), bk), s, m, B,
                                bs, ut, ht, d));
     return;
   }
@@ -316,7 +316,7 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
       constexpr size_t eb = eoe_stage_bytes<R, J, 2, 3>();
       const int bk = tuned_block(K_AD_EDGE);
       if (use_staged(m, B, V, eb, bk))
-        launch_k(k_ad_edge_st<R, A, V, J>, staged_cfg(m.nE, B, V, eb, bk), s, m, B, bs, ph, in, sd, w, (int)g_stable_base);
+        launch_k(ad_edge_st_kernel<R, A, V, J>(), staged_cfg(m.nE, B, V, eb, bk), s, m, B, bs, ph, in, sd, w, (int)g_stable_base);
       else
         launch_k(k_ad_edge<R, A, V, NB>, launch_cfg((long long)(m.nE) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
       break;
@@ -324,7 +324,7 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
     case 1: {
       const int bk = tuned_block(K_AD_CELL);
       if (use_staged(m, B, V, ad_cell_stage_bytes<R>(), bk))
-        launch_k(k_ad_cell_st<R, A, V>, staged_cfg(m.nC, B, V, ad_cell_stage_bytes<R>(), bk), s, m, B, bs, ph, in, sd,
+        launch_k(ad_cell_st_kernel<R, A, V>(), staged_cfg(m.nC, B, V, ad_cell_stage_bytes<R>(), bk), s, m, B, bs, ph, in, sd,
                  w, (int)g_stable_base);
       else
         launch_k(k_ad_cell<R, A, V, NB>, launch_cfg((long long)(m.nC) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
@@ -333,7 +333,7 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
     case 2: {
       const int bk = tuned_block(K_AD_VERTEX);
       if (use_staged(m, B, V, ad_vertex_stage_bytes<R>(), bk))
-        launch_k(k_ad_vertex_st<R, A, V>, staged_cfg(m.nV, B, V, ad_vertex_stage_bytes<R>(), bk), s, m, B, bs, ph, in,
+        launch_k(ad_vertex_st_kernel<R, A, V>(), staged_cfg(m.nV, B, V, ad_vertex_stage_bytes<R>(), bk), s, m, B, bs, ph, in,
                  sd, w);
       else
         launch_k(k_ad_vertex<R, A, V>, launch_cfg((long long)(m.nV) * ((B) / (V)), bk), s, m, B, bs, ph, in, sd, w);
@@ -348,7 +348,7 @@ static void ad_launch(int which, const MeshDev<R> &m, int B, const Base<R> &bs, 
         const long long cthreads = (long long)m.nC * (B / V);
         const int cell_blocks = (int)((cthreads + c.block - 1) / c.block);
         c.grid += cell_blocks;
-        launch_k(k_ad_final_st<R, A, V, J>, c, s, m, B, bs, ph, w, out, cell_blocks, (int)g_stable_base);
+        launch_k(ad_final_st_kernel<R, A, V, J>(), c, s, m, B, bs, ph, w, out, cell_blocks, (int)g_stable_base);
       } else {
         launch_k(k_ad_final<R, A, V, NB>, launch_cfg((long long)(m.nC + m.nE) * ((B) / (V)), bk), s, m, B, bs, ph, w, out);
       }

@@ -12,6 +12,33 @@
 
 namespace mpsw {
 
+// Register caps of the staged member kernels at 8 FP32 members per thread (the form the
+// autotuner picks on large meshes): each kernel X has a second form k_X_rc held to
+// MPSW_REGS_X registers, which X_kernel() selects for R = float, V = 8; 0 keeps the compiler's
+// own choice.  The values are the measured optimum on the level-7 mesh (occupancy against
+// in-flight loads per thread).
+#ifndef MPSW_REGS_TL_VERTEX
+#define MPSW_REGS_TL_VERTEX 32
+#endif
+#ifndef MPSW_REGS_TL_EDGE_DIAG
+#define MPSW_REGS_TL_EDGE_DIAG 64
+#endif
+#ifndef MPSW_REGS_TL_EDGE_TEND
+#define MPSW_REGS_TL_EDGE_TEND 64
+#endif
+#ifndef MPSW_REGS_AD_EDGE
+#define MPSW_REGS_AD_EDGE 56
+#endif
+#ifndef MPSW_REGS_AD_CELL
+#define MPSW_REGS_AD_CELL 0
+#endif
+#ifndef MPSW_REGS_AD_VERTEX
+#define MPSW_REGS_AD_VERTEX 0
+#endif
+#ifndef MPSW_REGS_AD_FINAL
+#define MPSW_REGS_AD_FINAL 40
+#endif
+
 // ---- V members of one entity -------------------------------------------------------------
 template <typename R, int V>
 struct alignas(sizeof(R) * V) Mv {
@@ -320,7 +347,7 @@ __host__ __device__ constexpr size_t vertex_stage_bytes() {
 // order; cell and kite) copied into shared memory before waiting for the previous kernel: they
 // are mesh data, which no kernel writes.  Same operations as k_tl_vertex.
 template <typename R, int V>
-__global__ void k_tl_vertex_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+__device__ __forceinline__ void tl_vertex_st_run(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
                                const R *__restrict__ ht, Diag<R> d) {
   using M = Mv<R, V>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -378,6 +405,27 @@ __global__ void k_tl_vertex_st(MeshDev<R> m, int B, Base<R> bs, const R *__restr
   if (d.vort) stv<V>(d.vort + o, vort);
   if (d.hv) stv<V>(d.hv + o, hvt);
   stv<V>(d.pvv + o, pvt);
+}
+template <typename R, int V>
+__global__ void k_tl_vertex_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                               const R *__restrict__ ht, Diag<R> d) {
+  tl_vertex_st_run<R, V>(m, B, bs, ut, ht, d);
+}
+#if MPSW_REGS_TL_VERTEX > 0
+template <int V>
+__global__ void __maxnreg__(MPSW_REGS_TL_VERTEX) k_tl_vertex_st_rc(MeshDev<float> m, int B, Base<float> bs, const float *__restrict__ ut,
+                               const float *__restrict__ ht, Diag<float> d) {
+  tl_vertex_st_run<float, V>(m, B, bs, ut, ht, d);
+}
+#endif
+template <typename R, int V>
+constexpr auto tl_vertex_st_kernel() {
+#if MPSW_REGS_TL_VERTEX > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_vertex_st_rc<V>;
+  else return &k_tl_vertex_st<R, V>;
+#else
+  return &k_tl_vertex_st<R, V>;
+#endif
 }
 
 // :274-316, :397-421, thickness tendency :541-561 and the RK update.  In FP32 the kernel is held
@@ -610,13 +658,23 @@ __global__ void k_tl_edge_diag_st(MeshDev<R> m, int B, Base<R> bs, const R *__re
                                   const R *__restrict__ ht, Diag<R> d, Phys<R> ph, int early) {
   tl_edge_diag_st_run<R, V, J>(m, B, bs, ut, ht, d, ph, early);
 }
-// FP32 at 8 members per thread held to 64 registers (4 blocks of 256 threads per SM instead of
-// 3 at the 72 it takes otherwise): measured 7% faster on level 7.
-template <int J>
-__global__ void __maxnreg__(64) k_tl_edge_diag_st_r64(MeshDev<float> m, int B, Base<float> bs,
-                                                      const float *__restrict__ ut, const float *__restrict__ ht,
-                                                      Diag<float> d, Phys<float> ph, int early) {
-  tl_edge_diag_st_run<float, 8, J>(m, B, bs, ut, ht, d, ph, early);
+#if MPSW_REGS_TL_EDGE_DIAG > 0
+template <int V, int J>
+__global__ void __maxnreg__(MPSW_REGS_TL_EDGE_DIAG) k_tl_edge_diag_st_rc(MeshDev<float> m, int B, Base<float> bs,
+                                                                        const float *__restrict__ ut,
+                                                                        const float *__restrict__ ht, Diag<float> d,
+                                                                        Phys<float> ph, int early) {
+  tl_edge_diag_st_run<float, V, J>(m, B, bs, ut, ht, d, ph, early);
+}
+#endif
+template <typename R, int V, int J>
+constexpr auto tl_edge_diag_st_kernel() {
+#if MPSW_REGS_TL_EDGE_DIAG > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_edge_diag_st_rc<V, J>;
+  else return &k_tl_edge_diag_st<R, V, J>;
+#else
+  return &k_tl_edge_diag_st<R, V, J>;
+#endif
 }
 
 // sw_compute_tend_tlm normal-velocity part :564-768 and the RK update.  Body for edge e,
@@ -728,26 +786,24 @@ __global__ void k_tl_edge_tend_st(MeshDev<R> m, int B, Base<R> bs, const R *__re
                                   R *tend_u, int early) {
   tl_edge_tend_st_run<R, A, V, J>(m, B, bs, ut, ht, d, ph, rk, tend_u, early);
 }
-// FP32 at 8 members per thread held to 64 registers (4 blocks of 256 threads per SM instead of
-// 3 at the 80 it takes otherwise): measured 11% faster on level 7.
-template <typename A, int J>
-__global__ void __maxnreg__(64) k_tl_edge_tend_st_r64(MeshDev<float> m, int B, Base<float> bs,
-                                                      const float *__restrict__ ut, const float *__restrict__ ht,
-                                                      Diag<float> d, Phys<float> ph, RK<float, A> rk,
-                                                      float *tend_u, int early) {
-  tl_edge_tend_st_run<float, A, 8, J>(m, B, bs, ut, ht, d, ph, rk, tend_u, early);
+#if MPSW_REGS_TL_EDGE_TEND > 0
+template <typename A, int V, int J>
+__global__ void __maxnreg__(MPSW_REGS_TL_EDGE_TEND) k_tl_edge_tend_st_rc(MeshDev<float> m, int B, Base<float> bs,
+                                                                        const float *__restrict__ ut,
+                                                                        const float *__restrict__ ht, Diag<float> d,
+                                                                        Phys<float> ph, RK<float, A> rk,
+                                                                        float *tend_u, int early) {
+  tl_edge_tend_st_run<float, A, V, J>(m, B, bs, ut, ht, d, ph, rk, tend_u, early);
 }
-
-// The staged edge kernels a launch uses: the 64-register forms for 8 FP32 members per thread.
-template <typename R, int V, int J>
-constexpr auto tl_edge_diag_st_kernel() {
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_edge_diag_st_r64<J>;
-  else return &k_tl_edge_diag_st<R, V, J>;
-}
+#endif
 template <typename R, typename A, int V, int J>
 constexpr auto tl_edge_tend_st_kernel() {
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_edge_tend_st_r64<A, J>;
+#if MPSW_REGS_TL_EDGE_TEND > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_edge_tend_st_rc<A, V, J>;
   else return &k_tl_edge_tend_st<R, A, V, J>;
+#else
+  return &k_tl_edge_tend_st<R, A, V, J>;
+#endif
 }
 
 // ----------------------------------------------------------------------------------------
@@ -873,7 +929,7 @@ __global__ void k_ad_edge(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> i
 // k_ad_edge with the edgesOnEdge lists (both weights; u, h_edge, pv_edge at the neighbours)
 // staged in shared memory: one block per epb edges.
 template <typename R, typename A, int V, int J>
-__global__ void k_ad_edge_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+__device__ __forceinline__ void ad_edge_st_run(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                              AdWork<R> w, int early) {
   if (!early) pdl_begin();
   int le, e, b;
@@ -883,6 +939,27 @@ __global__ void k_ad_edge_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R
   const EoeShared<R> st = stage_eoe<R, J, 2, 3>(m, blockIdx.x * epb, epb, le, fields);
   if (early) pdl_begin();
   if (mine) ad_edge_body<R, A, V, J>(m, B, bs, ph, in, sd, w, e, b, st);
+}
+template <typename R, typename A, int V, int J>
+__global__ void k_ad_edge_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+                             AdWork<R> w, int early) {
+  ad_edge_st_run<R, A, V, J>(m, B, bs, ph, in, sd, w, early);
+}
+#if MPSW_REGS_AD_EDGE > 0
+template <typename A, int V, int J>
+__global__ void __maxnreg__(MPSW_REGS_AD_EDGE) k_ad_edge_st_rc(MeshDev<float> m, int B, Base<float> bs, Phys<float> ph, AdIn<float> in, AdSeeds<float> sd,
+                             AdWork<float> w, int early) {
+  ad_edge_st_run<float, A, V, J>(m, B, bs, ph, in, sd, w, early);
+}
+#endif
+template <typename R, typename A, int V, int J>
+constexpr auto ad_edge_st_kernel() {
+#if MPSW_REGS_AD_EDGE > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_edge_st_rc<A, V, J>;
+  else return &k_ad_edge_st<R, A, V, J>;
+#else
+  return &k_ad_edge_st<R, A, V, J>;
+#endif
 }
 
 // del4 adjoint, first half (:588-634): delsq_vorticity/delsq_circulation adjoint on vertices
@@ -1000,7 +1077,7 @@ __host__ __device__ constexpr size_t ad_cell_stage_bytes() {
 // and zero coefficients, so every term there is an exact zero and all 6 slots run without a
 // bound check.  early: copy the lists before waiting for the previous kernel.
 template <typename R, typename A, int V>
-__global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd, AdWork<R> w,
+__device__ __forceinline__ void ad_cell_st_run(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd, AdWork<R> w,
                              int early) {
   using M = Mv<R, V>;
   constexpr int S = BoundsNarrow::c;
@@ -1073,6 +1150,27 @@ __global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R
   if (w.div_ad) stv<V>(w.div_ad + o, div_ad * (R(1) / area));
   stv<V>(w.hd + o, hd);
 }
+template <typename R, typename A, int V>
+__global__ void k_ad_cell_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd, AdWork<R> w,
+                             int early) {
+  ad_cell_st_run<R, A, V>(m, B, bs, ph, in, sd, w, early);
+}
+#if MPSW_REGS_AD_CELL > 0
+template <typename A, int V>
+__global__ void __maxnreg__(MPSW_REGS_AD_CELL) k_ad_cell_st_rc(MeshDev<float> m, int B, Base<float> bs, Phys<float> ph, AdIn<float> in, AdSeeds<float> sd, AdWork<float> w,
+                             int early) {
+  ad_cell_st_run<float, A, V>(m, B, bs, ph, in, sd, w, early);
+}
+#endif
+template <typename R, typename A, int V>
+constexpr auto ad_cell_st_kernel() {
+#if MPSW_REGS_AD_CELL > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_cell_st_rc<A, V>;
+  else return &k_ad_cell_st<R, A, V>;
+#else
+  return &k_ad_cell_st<R, A, V>;
+#endif
+}
 
 // Vertex stage: pv_cell -> pv_vertex (:215-229), pv_edge -> pv_vertex (:244-252),
 // gradPVt -> pv_vertex (:254-262), del2/del4 vorticity adjoints, pv_vertex -> h_vertex and
@@ -1135,7 +1233,7 @@ __host__ __device__ constexpr size_t ad_vertex_stage_bytes() {
 // shared memory before waiting for the previous kernel: they are mesh data, which no kernel
 // writes.  Same operations as k_ad_vertex.
 template <typename R, typename A, int V>
-__global__ void k_ad_vertex_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+__device__ __forceinline__ void ad_vertex_st_run(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
                                AdWork<R> w) {
   using M = Mv<R, V>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1208,6 +1306,27 @@ __global__ void k_ad_vertex_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn
   const size_t o = (size_t)v * B + b;
   stv<V>(w.hv_ad + o, hv_ad);
   stv<V>(w.circ_ad + o, circ_ad);
+}
+template <typename R, typename A, int V>
+__global__ void k_ad_vertex_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdIn<R> in, AdSeeds<R> sd,
+                               AdWork<R> w) {
+  ad_vertex_st_run<R, A, V>(m, B, bs, ph, in, sd, w);
+}
+#if MPSW_REGS_AD_VERTEX > 0
+template <typename A, int V>
+__global__ void __maxnreg__(MPSW_REGS_AD_VERTEX) k_ad_vertex_st_rc(MeshDev<float> m, int B, Base<float> bs, Phys<float> ph, AdIn<float> in, AdSeeds<float> sd,
+                               AdWork<float> w) {
+  ad_vertex_st_run<float, A, V>(m, B, bs, ph, in, sd, w);
+}
+#endif
+template <typename R, typename A, int V>
+constexpr auto ad_vertex_st_kernel() {
+#if MPSW_REGS_AD_VERTEX > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_vertex_st_rc<A, V>;
+  else return &k_ad_vertex_st<R, A, V>;
+#else
+  return &k_ad_vertex_st<R, A, V>;
+#endif
 }
 
 template <typename R, typename A, int V>
@@ -1347,7 +1466,7 @@ __global__ void k_ad_final(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWork<R
 // k_ad_final with staged edge lists: the first cell_blocks blocks take the cells (one member
 // group per thread), the others epb edges each with their lists in shared memory.
 template <typename R, typename A, int V, int J>
-__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWork<R> w, AdOut<R, A> out,
+__device__ __forceinline__ void ad_final_st_run(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWork<R> w, AdOut<R, A> out,
                               int cell_blocks, int early) {
   if ((int)blockIdx.x < cell_blocks) {
     pdl_begin();
@@ -1367,6 +1486,27 @@ __global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWor
   const EoeShared<R> st = stage_eoe<R, J, 2, 1>(m, ((int)blockIdx.x - cell_blocks) * epb, epb, le, fields);
   if (early) pdl_begin();
   if (le < epb && e < m.nE) ad_final_edge<R, A, V, J>(m, B, bs, ph, w, out, e, b, st);
+}
+template <typename R, typename A, int V, int J>
+__global__ void k_ad_final_st(MeshDev<R> m, int B, Base<R> bs, Phys<R> ph, AdWork<R> w, AdOut<R, A> out,
+                              int cell_blocks, int early) {
+  ad_final_st_run<R, A, V, J>(m, B, bs, ph, w, out, cell_blocks, early);
+}
+#if MPSW_REGS_AD_FINAL > 0
+template <typename A, int V, int J>
+__global__ void __maxnreg__(MPSW_REGS_AD_FINAL) k_ad_final_st_rc(MeshDev<float> m, int B, Base<float> bs, Phys<float> ph, AdWork<float> w, AdOut<float, A> out,
+                              int cell_blocks, int early) {
+  ad_final_st_run<float, A, V, J>(m, B, bs, ph, w, out, cell_blocks, early);
+}
+#endif
+template <typename R, typename A, int V, int J>
+constexpr auto ad_final_st_kernel() {
+#if MPSW_REGS_AD_FINAL > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_final_st_rc<A, V, J>;
+  else return &k_ad_final_st<R, A, V, J>;
+#else
+  return &k_ad_final_st<R, A, V, J>;
+#endif
 }
 
 }  // namespace mpsw
