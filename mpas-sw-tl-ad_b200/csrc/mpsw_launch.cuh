@@ -241,7 +241,7 @@ void Launch<R, A>::tl_cell(const MeshDev<R> &m, int B, const Base<R> &bs, const 
                                 tuned_v(K_TL_CELL));
   const int bk = tuned_block(K_TL_CELL);
   if (use_staged(m, B, v, cell_stage_bytes<R>(), bk)) {
-    MPSW_VDISPATCH(v, launch_k(k_tl_cell_st<R, A, VV>, staged_cfg(m.nC, B, VV, cell_stage_bytes<R>(), bk), s, m, B,
+    MPSW_VDISPATCH(v, launch_k(tl_cell_st_kernel<R, A, VV>(), staged_cfg(m.nC, B, VV, cell_stage_bytes<R>(), bk), s, m, B,
                                bs, ut, ht, d, rk, tend_h, (int)g_stable_base));
     return;
   }

@@ -20,6 +20,9 @@ namespace mpsw {
 #ifndef MPSW_REGS_TL_VERTEX
 #define MPSW_REGS_TL_VERTEX 32
 #endif
+#ifndef MPSW_REGS_TL_CELL
+#define MPSW_REGS_TL_CELL 72
+#endif
 #ifndef MPSW_REGS_TL_EDGE_DIAG
 #define MPSW_REGS_TL_EDGE_DIAG 64
 #endif
@@ -30,7 +33,7 @@ namespace mpsw {
 #define MPSW_REGS_AD_EDGE 56
 #endif
 #ifndef MPSW_REGS_AD_CELL
-#define MPSW_REGS_AD_CELL 0
+#define MPSW_REGS_AD_CELL 72
 #endif
 #ifndef MPSW_REGS_AD_VERTEX
 #define MPSW_REGS_AD_VERTEX 0
@@ -493,9 +496,9 @@ __host__ __device__ constexpr size_t cell_stage_bytes() {
 // there is an exact zero and all 6 slots run without a bound check.  early: copy the lists
 // before waiting for the previous kernel.
 template <typename R, typename A, int V>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
-    k_tl_cell_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut, const R *__restrict__ ht, Diag<R> d,
-                 RK<R, A> rk, R *tend_h, int early) {
+__device__ __forceinline__ void tl_cell_st_run(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut,
+                                               const R *__restrict__ ht, Diag<R> d, RK<R, A> rk, R *tend_h,
+                                               int early) {
   using M = Mv<R, V>;
   constexpr int S = BoundsNarrow::c;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -584,6 +587,31 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
   if (d.vc) stv<V>(d.vc + o, vc);
   if (tend_h) stv<V>(tend_h + o, th);
   rk_members<R, A, V>(rk, o, th);
+}
+template <typename R, typename A, int V>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
+    k_tl_cell_st(MeshDev<R> m, int B, Base<R> bs, const R *__restrict__ ut, const R *__restrict__ ht, Diag<R> d,
+                 RK<R, A> rk, R *tend_h, int early) {
+  tl_cell_st_run<R, A, V>(m, B, bs, ut, ht, d, rk, tend_h, early);
+}
+#if MPSW_REGS_TL_CELL > 0
+// (without the 48-register bound of the other forms)
+template <typename A, int V>
+__global__ void __maxnreg__(MPSW_REGS_TL_CELL) k_tl_cell_st_rc(MeshDev<float> m, int B, Base<float> bs,
+                                                              const float *__restrict__ ut,
+                                                              const float *__restrict__ ht, Diag<float> d,
+                                                              RK<float, A> rk, float *tend_h, int early) {
+  tl_cell_st_run<float, A, V>(m, B, bs, ut, ht, d, rk, tend_h, early);
+}
+#endif
+template <typename R, typename A, int V>
+constexpr auto tl_cell_st_kernel() {
+#if MPSW_REGS_TL_CELL > 0
+  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_cell_st_rc<A, V>;
+  else return &k_tl_cell_st<R, A, V>;
+#else
+  return &k_tl_cell_st<R, A, V>;
+#endif
 }
 
 // :319-329, :364-393, :425-445, h_edge_tl :117-126, delsq_u_tl :638-652.  Body for edge e,
