@@ -392,7 +392,7 @@ def fused_bytes(name, nC, nE, nV, B, s=4, a=8):
     return mesh + base + B * (E + C) * 4 * s
 
 
-def survey_stage_bytes(nC, nE, nV, sum_eoe, B, s=4, a=8):
+def model_stage_bytes(nC, nE, nV, sum_eoe, B, s=4, a=8):
     """The per-stage bytes M + B S of the path's algorithmic model: mesh read once per stage and,
     per member, x_k read and x_k+1 written at s, x0 read and the accumulator read and written at
     a: S = (N + E)(2 s + 3 a)."""
@@ -593,7 +593,7 @@ def run_mpsw(a, rank, world):
     top = max(cand, key=lambda k: kt[k])  # every candidate launches once per stage
     bytes_ = kbytes(top)
     ach = bytes_ / (kt[top] / 1e3) / 1e9
-    s8d = survey_stage_bytes(nC, nE, nV, sum_eoe, B)
+    s8d = model_stage_bytes(nC, nE, nV, sum_eoe, B)
     stages = {k: {'ms': kt[k], 'algorithmic_bytes': kbytes(k), 'achieved_gbs': kbytes(k) / (kt[k] / 1e3) / 1e9,
                   'frac': kbytes(k) / (kt[k] / 1e3) / 1e9 / hbm,
                   'frac_of_M_plus_BS': s8d / (kt[k] / 1e3) / 1e9 / hbm}
