@@ -8,6 +8,8 @@
 // does not change a single rounding (V = 1 is the single-member module path).
 #pragma once
 
+#include <cstdlib>
+
 #include "mpsw_kernels.cuh"
 
 namespace mpsw {
@@ -17,6 +19,12 @@ namespace mpsw {
 // MPSW_REGS_X registers, which X_kernel() selects for R = float, V = 8; 0 keeps the compiler's
 // own choice.  The values are the measured optimum on the level-7 mesh (occupancy against
 // in-flight loads per thread).
+// MPSW_REGCAP=0 launches the compiler's register choice instead (to measure the caps on other
+// meshes without a rebuild).
+inline bool regcap_on() {
+  static const bool on = !(std::getenv("MPSW_REGCAP") && std::atoi(std::getenv("MPSW_REGCAP")) == 0);
+  return on;
+}
 #ifndef MPSW_REGS_TL_VERTEX
 #define MPSW_REGS_TL_VERTEX 32
 #endif
@@ -422,9 +430,9 @@ __global__ void __maxnreg__(MPSW_REGS_TL_VERTEX) k_tl_vertex_st_rc(MeshDev<float
 }
 #endif
 template <typename R, int V>
-constexpr auto tl_vertex_st_kernel() {
+inline auto tl_vertex_st_kernel() {
 #if MPSW_REGS_TL_VERTEX > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_vertex_st_rc<V>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_tl_vertex_st_rc<V> : &k_tl_vertex_st<R, V>;
   else return &k_tl_vertex_st<R, V>;
 #else
   return &k_tl_vertex_st<R, V>;
@@ -605,9 +613,9 @@ __global__ void __maxnreg__(MPSW_REGS_TL_CELL) k_tl_cell_st_rc(MeshDev<float> m,
 }
 #endif
 template <typename R, typename A, int V>
-constexpr auto tl_cell_st_kernel() {
+inline auto tl_cell_st_kernel() {
 #if MPSW_REGS_TL_CELL > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_cell_st_rc<A, V>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_tl_cell_st_rc<A, V> : &k_tl_cell_st<R, A, V>;
   else return &k_tl_cell_st<R, A, V>;
 #else
   return &k_tl_cell_st<R, A, V>;
@@ -696,9 +704,9 @@ __global__ void __maxnreg__(MPSW_REGS_TL_EDGE_DIAG) k_tl_edge_diag_st_rc(MeshDev
 }
 #endif
 template <typename R, int V, int J>
-constexpr auto tl_edge_diag_st_kernel() {
+inline auto tl_edge_diag_st_kernel() {
 #if MPSW_REGS_TL_EDGE_DIAG > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_edge_diag_st_rc<V, J>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_tl_edge_diag_st_rc<V, J> : &k_tl_edge_diag_st<R, V, J>;
   else return &k_tl_edge_diag_st<R, V, J>;
 #else
   return &k_tl_edge_diag_st<R, V, J>;
@@ -825,9 +833,9 @@ __global__ void __maxnreg__(MPSW_REGS_TL_EDGE_TEND) k_tl_edge_tend_st_rc(MeshDev
 }
 #endif
 template <typename R, typename A, int V, int J>
-constexpr auto tl_edge_tend_st_kernel() {
+inline auto tl_edge_tend_st_kernel() {
 #if MPSW_REGS_TL_EDGE_TEND > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_tl_edge_tend_st_rc<A, V, J>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_tl_edge_tend_st_rc<A, V, J> : &k_tl_edge_tend_st<R, A, V, J>;
   else return &k_tl_edge_tend_st<R, A, V, J>;
 #else
   return &k_tl_edge_tend_st<R, A, V, J>;
@@ -981,9 +989,9 @@ __global__ void __maxnreg__(MPSW_REGS_AD_EDGE) k_ad_edge_st_rc(MeshDev<float> m,
 }
 #endif
 template <typename R, typename A, int V, int J>
-constexpr auto ad_edge_st_kernel() {
+inline auto ad_edge_st_kernel() {
 #if MPSW_REGS_AD_EDGE > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_edge_st_rc<A, V, J>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_ad_edge_st_rc<A, V, J> : &k_ad_edge_st<R, A, V, J>;
   else return &k_ad_edge_st<R, A, V, J>;
 #else
   return &k_ad_edge_st<R, A, V, J>;
@@ -1191,9 +1199,9 @@ __global__ void __maxnreg__(MPSW_REGS_AD_CELL) k_ad_cell_st_rc(MeshDev<float> m,
 }
 #endif
 template <typename R, typename A, int V>
-constexpr auto ad_cell_st_kernel() {
+inline auto ad_cell_st_kernel() {
 #if MPSW_REGS_AD_CELL > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_cell_st_rc<A, V>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_ad_cell_st_rc<A, V> : &k_ad_cell_st<R, A, V>;
   else return &k_ad_cell_st<R, A, V>;
 #else
   return &k_ad_cell_st<R, A, V>;
@@ -1348,9 +1356,9 @@ __global__ void __maxnreg__(MPSW_REGS_AD_VERTEX) k_ad_vertex_st_rc(MeshDev<float
 }
 #endif
 template <typename R, typename A, int V>
-constexpr auto ad_vertex_st_kernel() {
+inline auto ad_vertex_st_kernel() {
 #if MPSW_REGS_AD_VERTEX > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_vertex_st_rc<A, V>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_ad_vertex_st_rc<A, V> : &k_ad_vertex_st<R, A, V>;
   else return &k_ad_vertex_st<R, A, V>;
 #else
   return &k_ad_vertex_st<R, A, V>;
@@ -1528,9 +1536,9 @@ __global__ void __maxnreg__(MPSW_REGS_AD_FINAL) k_ad_final_st_rc(MeshDev<float> 
 }
 #endif
 template <typename R, typename A, int V, int J>
-constexpr auto ad_final_st_kernel() {
+inline auto ad_final_st_kernel() {
 #if MPSW_REGS_AD_FINAL > 0
-  if constexpr (std::is_same<R, float>::value && V == 8) return &k_ad_final_st_rc<A, V, J>;
+  if constexpr (std::is_same<R, float>::value && V == 8) return regcap_on() ? &k_ad_final_st_rc<A, V, J> : &k_ad_final_st<R, A, V, J>;
   else return &k_ad_final_st<R, A, V, J>;
 #else
   return &k_ad_final_st<R, A, V, J>;
